@@ -1,0 +1,332 @@
+"""Benchmark: CBM D^-1/2 A D^-1/2 X throughput (GB/s of algorithmic bytes) on B200.
+
+Workload (default): the 1,000,000-node power-law graph (Chung-Lu exponent 2.1,
+mean degree 20, 30% near-duplicate rows with 10% flips, symmetrised, seed 1),
+CBM built with alpha = 8, X 1e6 x 256 fp32 N(0,1); one step = one
+D^-1/2 A D^-1/2 X product (cbm4dad.matmul).  X and Y (1.02 GB each) exceed
+the 126 MB L2, so no flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+N > 1 runs under torchrun, one rank per GPU: each rank owns a 256-column shard
+of X and Y (column sharding needs no collective; weak scaling).  Rank 0
+prints one JSON line.  ``--impl reference`` times the reference's CPU product
+path (CSR SpMM + branch-serial fused update, cbm/cbm_extensions.cpp:593-698) as
+restated by the oracle, on all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+import torch
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "cbm-gpu_b200"))
+
+WORKLOAD = "powerlaw-1m"
+COLS = 256
+HBM_FALLBACK_GBS = 6650.0
+
+
+def peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+def bytes_alg(n, z, e, b, cols, sx=4, sy=4, scaled=True):
+    """Algorithmic bytes of one product: row pointers + column indices, one X-row
+    gather per delta entry, Y written once, per tree edge its ids and one fp32
+    parent-row read, branch offsets, and the D^-1/2 vector."""
+    return (4 * (n + 1) + 4 * z + z * cols * sx + n * cols * sy + e * (8 + 4 * cols) + 4 * (b + 1)
+            + (4 * n if scaled else 0))
+
+
+def load_graph(rank, world):
+    """Edge list + CBM structure, built once and shared through a file cache."""
+    from cbm import cbm_mkl_cpp, synthetic
+
+    cache = os.path.join(REPO, "_cache")
+    os.makedirs(cache, exist_ok=True)
+    path = os.path.join(cache, f"{WORKLOAD}.npz")
+    if rank == 0 and not os.path.exists(path):
+        ei, n, spec = synthetic.workload(WORKLOAD)
+        np.savez(path + ".tmp.npz", ei=ei, n=n)
+        os.replace(path + ".tmp.npz", path)
+    if world > 1:
+        torch.distributed.barrier()
+    d = np.load(path)
+    return d["ei"], int(d["n"]), synthetic.WORKLOADS[WORKLOAD]
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        for line in (self.out or "").splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), float(parts[3]), parts[5:9]))
+            except ValueError:
+                continue
+        if not rows:
+            return None
+        loaded = [r for r in rows if r[2] > 200.0] or rows
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in loaded for i, v in enumerate(r[3]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in loaded), "sm_max_mhz": max(r[1] for r in rows),
+                "samples": len(rows), "reasons": reasons}
+
+
+def traffic_from_profile():
+    """DRAM bytes per launch of the product kernel from the committed ncu summary."""
+    path = os.path.join(REPO, "profiles", "fwd_kernel_powerlaw-1m.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+def cpu_baseline(a, x_np, b_alg, budget_s=15.0):
+    """The reference's CPU product path (oracle port, all threads) on the same workload."""
+    from oracle import oracle
+
+    crow = a.deltas.crow_indices().cpu().numpy()
+    col = a.deltas.col_indices().cpu().numpy()
+    val = a.deltas.values().cpu().numpy()
+    br, src, dst = (t.cpu().numpy() for t in (a.mca_offset, a.mca_src_idx, a.mca_dst_idx))
+    mult = a.D.cpu().numpy()
+    times = []
+    t_end = time.perf_counter() + budget_s
+    while not times or time.perf_counter() < t_end:
+        t0 = time.perf_counter()
+        oracle.spmm_fused_update(crow, col, val, x_np, br, src, dst, mult, parallel=True)
+        times.append(time.perf_counter() - t0)
+        if len(times) >= 5:
+            break
+    t = statistics.median(times)
+    return {"value": b_alg / t / 1e9, "unit": "GB/s", "cores": oracle.threads(), "kind": "port",
+            "sample": f"{len(times)} full products (median {t:.2f} s) of the same workload on the host CPU"}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's CPU product path timed on the host cores."""
+    if rank != 0:
+        return
+    from cbm import cbm_mkl_cpp
+    from oracle import oracle
+
+    ei, n, spec = load_graph(0, 1)
+    s = cbm_mkl_cpp.build(ei[0], ei[1], n, spec["alpha"])
+    crow, col = s.csr_ptr, s.csr_col
+    deg = np.diff(oracle.csr_from_edges(ei, n)[0]).astype(np.float32)
+    with np.errstate(divide="ignore"):
+        dinv = (1.0 / np.sqrt(deg)).astype(np.float32)
+    rows = np.repeat(np.arange(n), np.diff(crow))
+    val = (s.csr_val * dinv[col]) * dinv[rows]
+    x = np.random.default_rng(1).standard_normal((n, COLS), dtype=np.float32)
+    z, e, b = int(col.size), int(s.src.size), int(s.branches.size) - 1
+    b_alg = bytes_alg(n, z, e, b, COLS)
+    for _ in range(args.warmup):
+        oracle.spmm_fused_update(crow, col, val, x, s.branches, s.src, s.dst, dinv, parallel=True)
+    ts = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        oracle.spmm_fused_update(crow, col, val, x, s.branches, s.src, s.dst, dinv, parallel=True)
+        ts.append(time.perf_counter() - t0)
+    t = sum(ts) / len(ts)
+    v = b_alg / t / 1e9
+    cores = oracle.threads()
+    line = {"impl": "reference", "metric": "CBM DAD.X GB/s (algorithmic bytes)", "value": v, "unit": "GB/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": config_dict(n, s.nnz_a, z, e, b, world),
+            "cpu_baseline": {"value": v, "unit": "GB/s", "cores": cores, "kind": "port",
+                             "sample": "every step one full product of the workload (oracle port of "
+                                       "s_spmm_fused_update_csr_int32, OpenMP)"},
+            "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def config_dict(n, nnz_a, z, e, b, world):
+    return {"workload": f"{WORKLOAD}: D^-1/2 A D^-1/2 X fp32, power-law N={n}, alpha=8, C={COLS} per GPU",
+            "nodes": n, "nnz_a": nnz_a, "nnz_delta": z, "tree_edges": e, "branches": b, "cols_per_gpu": COLS,
+            "l2": "inputs larger than L2 (X and Y 1.02 GB each), no flush", "parallelism": f"column shards x{world}"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        torch.cuda.set_device(local)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                             device_id=torch.device("cuda", local))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
+
+    from cbm import _lib
+    from cbm.cbm4dad import cbm4dad
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    ei, n, spec = load_graph(rank, world)
+    a = cbm4dad(torch.from_numpy(ei), torch.ones(ei.shape[1]), alpha=spec["alpha"])
+    st = a.plan.stats
+    z, e, b = st["nnz"], st["edges"], st["branches"]
+    b_alg = bytes_alg(n, z, e, b, COLS)
+
+    g = torch.Generator(device=dev).manual_seed(1 + rank)
+    x = torch.randn(n, COLS, device=dev, generator=g)
+    y = torch.empty(n, COLS, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize(dev)
+
+    # ---- device-timed product (inputs resident in HBM) ----
+    for _ in range(args.warmup):
+        a.matmul(x, y)
+    barrier()
+    launches0 = a.plan.stat(_lib.P_LAUNCHES)
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    with Clocks(local) as clk:
+        barrier()
+        evs[0].record(stream)
+        for i in range(args.steps):
+            a.matmul(x, y)
+            evs[i + 1].record(stream)
+        barrier()
+    launches = a.plan.stat(_lib.P_LAUNCHES) - launches0
+    per = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
+    ms = evs[0].elapsed_time(evs[-1]) / args.steps
+    ms_all = torch.tensor([ms], device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(ms_all, op=torch.distributed.ReduceOp.MAX)
+    ms_max = float(ms_all.item())
+    a.plan.check_device()
+
+    # ---- end to end through the public API with host buffers ----
+    xh = torch.empty(n, COLS, dtype=torch.float32, pin_memory=True)
+    xh.copy_(x.cpu())
+    yh = torch.empty(n, COLS, dtype=torch.float32, pin_memory=True)
+    xd = torch.empty_like(x)
+    e2e_steps = max(3, min(args.steps, 10))
+    for _ in range(2):
+        xd.copy_(xh, non_blocking=True)
+        a.matmul(xd, y)
+        yh.copy_(y, non_blocking=True)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        xd.copy_(xh, non_blocking=True)
+        a.matmul(xd, y)
+        yh.copy_(y, non_blocking=True)
+    e1.record(stream)
+    barrier()
+    e2e_ms = torch.tensor([e0.elapsed_time(e1) / e2e_steps], device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(e2e_ms, op=torch.distributed.ReduceOp.MAX)
+    e2e_ms = float(e2e_ms.item())
+
+    if rank == 0:
+        peak, peak_kind = peaks()
+        kernel_ms = statistics.mean(per)
+        achieved = b_alg / (kernel_ms * 1e-3) / 1e9
+        line = {
+            "metric": "CBM DAD.X GB/s (algorithmic bytes)",
+            "value": b_alg * world / (ms_max * 1e-3) / 1e9,
+            "unit": "GB/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_max,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic",
+            "config": config_dict(n, a.structure_stats["nnz_a"], z, e, b, world),
+            "rows_per_s": n * world / (ms_max * 1e-3),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic_from_profile(),
+                         "kernel": "cbm::fwd_kernel<float,float,2,4>", "bytes_alg_per_launch": b_alg},
+            "e2e": {"value": b_alg * world / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s",
+                    "h2d_bytes_per_step": int(xh.numel() * 4), "d2h_bytes_per_step": int(yh.numel() * 4),
+                    "ms_per_step": e2e_ms},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+            "plan": st,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(a, x.cpu().numpy(), b_alg)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,63 @@
+"""``cbm4mm``: A stored in CBM form, products Y = A X (cbm/cbm4mm.py:7-54).
+
+Same constructor arguments (edge_index int32 [2, nnz], edge_values float32
+[nnz], alpha) and attributes (deltas, num_nodes, mca_offset, mca_src_idx,
+mca_dst_idx, cusparse_extension) as the reference class.  ``matmul(x, y)``
+writes A x into the preallocated y, on the current stream.
+
+Beyond the reference: x may be bfloat16 (y float32 or bfloat16, FP32
+accumulation), ``forward(x)`` is differentiable through torch.autograd
+(the adjoint runs in CBM form), and ``adjoint(g, dx)`` computes A^T g.
+"""
+from __future__ import annotations
+
+import torch
+
+from . import cbm_mkl_cpp as cbm_mkl
+from .cbm_cusparse import cusparseCBM
+from .plan import Plan
+
+__all__ = ["cbm4mm"]
+
+
+class cbm4mm:  # noqa: N801 (the reference's class name)
+    _op = "ax"
+
+    def __init__(self, edge_index, edge_values, alpha=0):
+        if edge_index.numel() == 0:
+            raise RuntimeError("edge_index is empty")
+        num_rows = int(max(edge_index[0].max(), edge_index[1].max())) + 1
+        if isinstance(edge_values, torch.Tensor) and edge_values.dtype != torch.float32:
+            raise RuntimeError('"src_values" is not a tensor of type "torch::kFloat32"')
+        s = cbm_mkl.build(edge_index[0], edge_index[1], num_rows, alpha)
+        self.structure_stats = {"nnz_a": s.nnz_a, "nnz_delta": int(s.csr_col.size), "edges": int(s.src.size),
+                                "branches": int(s.branches.size) - 1, "candidates": s.n_candidates}
+        self.deltas = torch.sparse_csr_tensor(
+            torch.from_numpy(s.csr_ptr), torch.from_numpy(s.csr_col), torch.from_numpy(s.csr_val),
+            (num_rows, num_rows)).to(device="cuda")
+        self.num_nodes = num_rows
+        self.mca_offset = torch.from_numpy(s.branches).to(dtype=torch.int32, device="cuda")
+        self.mca_src_idx = torch.from_numpy(s.src).to(dtype=torch.int32, device="cuda")
+        self.mca_dst_idx = torch.from_numpy(s.dst).to(dtype=torch.int32, device="cuda")
+        self.parent = s.parent  # host int32 [N], N = virtual root
+        self._plan = Plan(s.csr_ptr, s.csr_col, s.csr_val, num_rows, num_rows, s.branches, s.src, s.dst,
+                          host=True)
+        self.cusparse_extension = cusparseCBM._from_plan(self._plan, "ax", None, False)
+
+    @property
+    def plan(self):
+        return self._plan
+
+    def matmul(self, x, y):
+        self._plan.matmul(self._op, x, y)
+
+    def adjoint(self, g, dx):
+        """dx <- (this operator)^T g."""
+        self._plan.adjoint(self._op, g, dx)
+
+    def forward(self, x, out_dtype=None):
+        """Differentiable y = (this operator) x; y has x's dtype unless out_dtype is given."""
+        from .autograd import cbm_apply
+        return cbm_apply(self, x, out_dtype)
+
+    __call__ = forward

@@ -1,0 +1,492 @@
+// Launch side of the CBM product: operand checks, tile-shape selection and the
+// kernel instantiations behind cbm_matmul / cbm_matmul_adjoint.
+
+#include "cbm_b200.h"
+#include "kernels.cuh"
+#include "plan.h"
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+namespace cbm {
+namespace {
+
+int sm_count(int device) {
+  static int cached_dev = -1, cached = 0;
+  if (cached_dev != device) {
+    cudaDeviceGetAttribute(&cached, cudaDevAttrMultiProcessorCount, device);
+    cached_dev = device;
+  }
+  return cached > 0 ? cached : 1;
+}
+
+template <typename K>
+int grid_for(K kernel, int device) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, 0) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  return per_sm * sm_count(device);
+}
+
+int64_t round4(int64_t x) { return (x + 3) / 4 * 4; }
+int64_t align256(int64_t b) { return (b + 255) / 256 * 256; }
+
+// Columns one launch covers: 32 lanes x 8 vectors x V elements.
+int64_t block_cols(int v) { return 32 * 8 * (int64_t)v; }
+
+struct Shape {
+  bool vec;
+  int v;       // elements per vector
+  int64_t cb;  // columns per launch
+};
+
+int elem_size(int32_t dt) { return dt == CBM_BF16 ? 2 : 4; }
+
+Shape pick_shape(int32_t xdt, int32_t ydt, const void* x, int64_t ldx, const void* y, int64_t ldy, int64_t c) {
+  const int vv = xdt == CBM_BF16 ? 8 : 4;
+  const bool aligned = c % vv == 0 && (reinterpret_cast<uintptr_t>(x) % 16 == 0) &&
+                       (reinterpret_cast<uintptr_t>(y) % 16 == 0) && (ldx * elem_size(xdt)) % 16 == 0 &&
+                       (ldy * elem_size(ydt)) % 16 == 0;
+  Shape s;
+  s.vec = aligned;
+  s.v = aligned ? vv : 1;
+  s.cb = block_cols(s.v);
+  return s;
+}
+
+void team_for(int64_t nvec, int* team, int* vpl) {
+  if (nvec >= 32) {
+    *team = 32;
+    const int64_t need = (nvec + 31) / 32;
+    *vpl = need <= 1 ? 1 : need <= 2 ? 2 : need <= 4 ? 4 : 8;
+  } else {
+    int t = 1;
+    while (t < nvec) t <<= 1;
+    *team = t;
+    *vpl = 1;
+  }
+}
+
+bool dtype_ok(int32_t xdt, int32_t ydt) {
+  return (xdt == CBM_F32 && ydt == CBM_F32) || (xdt == CBM_BF16 && ydt == CBM_F32) ||
+         (xdt == CBM_BF16 && ydt == CBM_BF16);
+}
+
+bool overlaps(const void* a, int64_t abytes, const void* b, int64_t bbytes) {
+  const uintptr_t a0 = reinterpret_cast<uintptr_t>(a), b0 = reinterpret_cast<uintptr_t>(b);
+  return a0 < b0 + (uintptr_t)bbytes && b0 < a0 + (uintptr_t)abytes;
+}
+
+// ---- forward launch ------------------------------------------------------------
+template <typename XT, typename YT, int VPL, int V>
+int launch_fwd_t(cbm_plan* P, const FwdArgs& a, cudaStream_t st) {
+  static int grid_cache = 0, grid_dev = -1;
+  if (grid_dev != P->device) {
+    grid_cache = grid_for(fwd_kernel<XT, YT, VPL, V>, P->device);
+    grid_dev = P->device;
+  }
+  fwd_kernel<XT, YT, VPL, V><<<grid_cache, kThreads, 0, st>>>(a);
+  P->launches++;
+  P->last_grid = grid_cache;
+  return cuda_status(cudaGetLastError());
+}
+
+template <typename XT, typename YT, int V>
+int launch_fwd_v(cbm_plan* P, const FwdArgs& a, int vpl, cudaStream_t st) {
+  switch (vpl) {
+    case 1: return launch_fwd_t<XT, YT, 1, V>(P, a, st);
+    case 2: return launch_fwd_t<XT, YT, 2, V>(P, a, st);
+    case 4: return launch_fwd_t<XT, YT, 4, V>(P, a, st);
+    default: return launch_fwd_t<XT, YT, 8, V>(P, a, st);
+  }
+}
+
+int launch_fwd(cbm_plan* P, const FwdArgs& a, int32_t xdt, int32_t ydt, bool vec, int vpl, cudaStream_t st) {
+  if (xdt == CBM_F32) {
+    return vec ? launch_fwd_v<float, float, 4>(P, a, vpl, st) : launch_fwd_v<float, float, 1>(P, a, vpl, st);
+  }
+  if (ydt == CBM_F32) {
+    return vec ? launch_fwd_v<__nv_bfloat16, float, 8>(P, a, vpl, st)
+               : launch_fwd_v<__nv_bfloat16, float, 1>(P, a, vpl, st);
+  }
+  return vec ? launch_fwd_v<__nv_bfloat16, __nv_bfloat16, 8>(P, a, vpl, st)
+             : launch_fwd_v<__nv_bfloat16, __nv_bfloat16, 1>(P, a, vpl, st);
+}
+
+// ---- adjoint launches -------------------------------------------------------------
+template <typename GT, int VPL, int V>
+int launch_rev_t(cbm_plan* P, const RevArgs& a, cudaStream_t st) {
+  static int grid_cache = 0, grid_dev = -1;
+  if (grid_dev != P->device) {
+    grid_cache = grid_for(rev_kernel<GT, VPL, V>, P->device);
+    grid_dev = P->device;
+  }
+  rev_kernel<GT, VPL, V><<<grid_cache, kThreads, 0, st>>>(a);
+  P->launches++;
+  return cuda_status(cudaGetLastError());
+}
+template <typename GT, typename DT, int VPL, int V>
+int launch_tr_t(cbm_plan* P, const TrArgs& a, cudaStream_t st) {
+  static int grid_cache = 0, grid_dev = -1;
+  if (grid_dev != P->device) {
+    grid_cache = grid_for(tr_kernel<GT, DT, VPL, V>, P->device);
+    grid_dev = P->device;
+  }
+  tr_kernel<GT, DT, VPL, V><<<grid_cache, kThreads, 0, st>>>(a);
+  P->launches++;
+  return cuda_status(cudaGetLastError());
+}
+template <typename GT, int V>
+int launch_rev_v(cbm_plan* P, const RevArgs& a, int vpl, cudaStream_t st) {
+  switch (vpl) {
+    case 1: return launch_rev_t<GT, 1, V>(P, a, st);
+    case 2: return launch_rev_t<GT, 2, V>(P, a, st);
+    case 4: return launch_rev_t<GT, 4, V>(P, a, st);
+    default: return launch_rev_t<GT, 8, V>(P, a, st);
+  }
+}
+template <typename GT, typename DT, int V>
+int launch_tr_v(cbm_plan* P, const TrArgs& a, int vpl, cudaStream_t st) {
+  switch (vpl) {
+    case 1: return launch_tr_t<GT, DT, 1, V>(P, a, st);
+    case 2: return launch_tr_t<GT, DT, 2, V>(P, a, st);
+    case 4: return launch_tr_t<GT, DT, 4, V>(P, a, st);
+    default: return launch_tr_t<GT, DT, 8, V>(P, a, st);
+  }
+}
+int launch_rev(cbm_plan* P, const RevArgs& a, int32_t gdt, bool vec, int vpl, cudaStream_t st) {
+  if (gdt == CBM_F32) return vec ? launch_rev_v<float, 4>(P, a, vpl, st) : launch_rev_v<float, 1>(P, a, vpl, st);
+  return vec ? launch_rev_v<__nv_bfloat16, 8>(P, a, vpl, st) : launch_rev_v<__nv_bfloat16, 1>(P, a, vpl, st);
+}
+int launch_tr(cbm_plan* P, const TrArgs& a, int32_t gdt, int32_t ddt, bool vec, int vpl, cudaStream_t st) {
+  if (gdt == CBM_F32) {
+    return vec ? launch_tr_v<float, float, 4>(P, a, vpl, st) : launch_tr_v<float, float, 1>(P, a, vpl, st);
+  }
+  if (ddt == CBM_F32) {
+    return vec ? launch_tr_v<__nv_bfloat16, float, 8>(P, a, vpl, st)
+               : launch_tr_v<__nv_bfloat16, float, 1>(P, a, vpl, st);
+  }
+  return vec ? launch_tr_v<__nv_bfloat16, __nv_bfloat16, 8>(P, a, vpl, st)
+             : launch_tr_v<__nv_bfloat16, __nv_bfloat16, 1>(P, a, vpl, st);
+}
+
+template <typename T>
+int upload(T** dst, const std::vector<T>& src, cudaStream_t st, std::vector<void*>& owned) {
+  *dst = nullptr;
+  if (src.empty()) return CBM_OK;
+  void* p = nullptr;
+  if (cudaMalloc(&p, src.size() * sizeof(T)) != cudaSuccess) return CBM_ERR_ALLOC;
+  owned.push_back(p);
+  if (cudaMemcpyAsync(p, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, st) != cudaSuccess)
+    return CBM_ERR_CUDA;
+  *dst = static_cast<T*>(p);
+  return CBM_OK;
+}
+
+int zeros_u32(unsigned** dst, int64_t n, cudaStream_t st, std::vector<void*>& owned) {
+  *dst = nullptr;
+  if (n <= 0) return CBM_OK;
+  void* p = nullptr;
+  if (cudaMalloc(&p, n * sizeof(unsigned)) != cudaSuccess) return CBM_ERR_ALLOC;
+  owned.push_back(p);
+  if (cudaMemsetAsync(p, 0, n * sizeof(unsigned), st) != cudaSuccess) return CBM_ERR_CUDA;
+  *dst = static_cast<unsigned*>(p);
+  return CBM_OK;
+}
+
+}  // namespace
+
+int rebuild_adjoint_chunks(cbm_plan* P, cudaStream_t st) {
+  if (!P->adj_built) return CBM_OK;
+  free_all(P->adj_chunk_bufs);
+  std::vector<int32_t> chunk0(P->n_cols, -1), citem;
+  std::vector<int64_t> cbeg, cend;
+  const int64_t T = P->chunk_nnz;
+  for (int64_t j = 0; j < P->n_cols; ++j) {
+    const int64_t b = P->h_t_ptr[j], e = P->h_t_ptr[j + 1];
+    if (e - b > T) {
+      chunk0[j] = (int32_t)citem.size();
+      for (int64_t s = b; s < e; s += T) {
+        citem.push_back((int32_t)j);
+        cbeg.push_back(s);
+        cend.push_back(std::min(e, s + T));
+      }
+    }
+  }
+  P->n_t_chunks = (int64_t)citem.size();
+  int rc;
+  if ((rc = upload(&P->d_t_chunk0, chunk0, st, P->adj_chunk_bufs))) return rc;
+  if ((rc = upload(&P->d_t_chunk_item, citem, st, P->adj_chunk_bufs))) return rc;
+  if ((rc = upload(&P->d_t_chunk_beg, cbeg, st, P->adj_chunk_bufs))) return rc;
+  if ((rc = upload(&P->d_t_chunk_end, cend, st, P->adj_chunk_bufs))) return rc;
+  if ((rc = zeros_u32(&P->d_t_chunk_flag, P->n_t_chunks, st, P->adj_chunk_bufs))) return rc;
+  return cuda_status(cudaStreamSynchronize(st));
+}
+
+// Reverse-propagation items (internal nodes, deepest first, with their
+// children) and the transposed delta matrix, both built once on the host.
+int build_adjoint(cbm_plan* P, cudaStream_t st) {
+  if (P->adj_built) return CBM_OK;
+  if (P->n_rows >= (int64_t)kInternalBit || P->n_cols >= (int64_t)kInternalBit) return CBM_ERR_INVALID;
+  const int64_t n = P->n_rows;
+  // children lists, by parent
+  std::vector<int64_t> cptr(n + 1, 0);
+  for (int64_t v = 0; v < n; ++v)
+    if (P->h_parent[v] >= 0) cptr[P->h_parent[v] + 1]++;
+  for (int64_t v = 0; v < n; ++v) cptr[v + 1] += cptr[v];
+  std::vector<int32_t> kids(cptr[n]);
+  {
+    std::vector<int64_t> fill(cptr.begin(), cptr.end() - 1);
+    for (int64_t v = 0; v < n; ++v)
+      if (P->h_parent[v] >= 0) kids[fill[P->h_parent[v]]++] = (int32_t)v;
+  }
+  // internal nodes in reverse item (level) order
+  std::vector<int32_t> rnode, rslot;
+  std::vector<int64_t> rptr(1, 0);
+  std::vector<uint32_t> rent;
+  for (int64_t i = n - 1; i >= 0; --i) {
+    const int32_t w = P->h_order[i];
+    if (P->h_slot[w] < 0) continue;
+    rnode.push_back(w);
+    rslot.push_back(P->h_slot[w]);
+    for (int64_t k = cptr[w]; k < cptr[w + 1]; ++k) {
+      const int32_t c = kids[k];
+      rent.push_back(P->h_slot[c] >= 0 ? ((uint32_t)P->h_slot[c] | kInternalBit) : (uint32_t)c);
+    }
+    rptr.push_back((int64_t)rent.size());
+  }
+  // transposed delta: column j lists (row v or its slot, sign)
+  P->h_t_ptr.assign(P->n_cols + 1, 0);
+  for (int64_t k = 0; k < P->nnz; ++k) P->h_t_ptr[(P->h_ent[k] & 0x7fffffffu) + 1]++;
+  for (int64_t j = 0; j < P->n_cols; ++j) P->h_t_ptr[j + 1] += P->h_t_ptr[j];
+  std::vector<uint32_t> tent(P->nnz);
+  {
+    std::vector<int64_t> fill(P->h_t_ptr.begin(), P->h_t_ptr.end() - 1);
+    // visit rows in node order so each column's list is sorted by row
+    std::vector<int64_t> item_of(n);
+    for (int64_t i = 0; i < n; ++i) item_of[P->h_order[i]] = i;
+    for (int64_t v = 0; v < n; ++v) {
+      const int64_t i = item_of[v];
+      const uint32_t rv = P->h_slot[v] >= 0 ? ((uint32_t)P->h_slot[v] | kInternalBit) : (uint32_t)v;
+      for (int64_t k = P->h_ptr[i]; k < P->h_ptr[i + 1]; ++k) {
+        const uint32_t e = P->h_ent[k];
+        tent[fill[e & 0x7fffffffu]++] = rv | (e & 0x80000000u);
+      }
+    }
+  }
+  int rc;
+  if ((rc = upload(&P->d_rev_node, rnode, st, P->adj_bufs))) return rc;
+  if ((rc = upload(&P->d_rev_slot, rslot, st, P->adj_bufs))) return rc;
+  if ((rc = upload(&P->d_rev_ptr, rptr, st, P->adj_bufs))) return rc;
+  if ((rc = upload(&P->d_rev_ent, rent, st, P->adj_bufs))) return rc;
+  if ((rc = zeros_u32(&P->d_adj_flag, P->n_internal, st, P->adj_bufs))) return rc;
+  if ((rc = upload(&P->d_t_ptr, P->h_t_ptr, st, P->adj_bufs))) return rc;
+  if ((rc = upload(&P->d_t_ent, tent, st, P->adj_bufs))) return rc;
+  P->adj_built = true;
+  return rebuild_adjoint_chunks(P, st);
+}
+
+}  // namespace cbm
+
+using namespace cbm;
+
+extern "C" {
+
+int64_t cbm_plan_workspace_bytes(const cbm_plan* P, int32_t op, int64_t n_cols, int32_t x_dtype, int32_t y_dtype,
+                                 int32_t adjoint) {
+  if (!P || n_cols < 0) return -1;
+  (void)op;
+  const int vv = x_dtype == CBM_BF16 ? 8 : 4;
+  const int64_t cols = std::min<int64_t>(n_cols, block_cols(vv));
+  const int64_t ldp = round4(cols);
+  int64_t rows;
+  if (adjoint) {
+    // chunk counts of the transposed matrix are only known once built; bound
+    // them by nnz / chunk_nnz + n_cols
+    const int64_t t_chunks = P->adj_built ? P->n_t_chunks : (2 * P->nnz / P->chunk_nnz + 1);
+    rows = P->n_internal + t_chunks;
+  } else {
+    rows = P->n_chunks + (y_dtype == CBM_BF16 ? P->n_internal : 0);
+  }
+  return align256(rows * ldp * 4) + 256;
+}
+
+int cbm_plan_set_timeout(cbm_plan* P, int64_t ns) {
+  if (!P || ns <= 0) return CBM_ERR_INVALID;
+  P->timeout_ns = ns;
+  return CBM_OK;
+}
+
+int cbm_plan_debug_set_parent(cbm_plan* P, int64_t item, int32_t parent_node, void* stream) {
+  // Test hook: points an item's parent at another node (e.g. a leaf, whose
+  // ready flag nothing sets) so that the bounded wait can be exercised.
+  if (!P || item < 0 || item >= P->n_items || parent_node < -1 || parent_node >= P->n_rows) return CBM_ERR_INVALID;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (cudaMemcpyAsync(P->d_par + item, &parent_node, sizeof(int32_t), cudaMemcpyHostToDevice, st) != cudaSuccess)
+    return CBM_ERR_CUDA;
+  const int32_t zero = 0;
+  if (cudaMemcpyAsync(P->d_par_slot + item, &zero, sizeof(int32_t), cudaMemcpyHostToDevice, st) != cudaSuccess)
+    return CBM_ERR_CUDA;
+  return cuda_status(cudaStreamSynchronize(st));
+}
+
+int cbm_matmul(cbm_plan* P, int32_t op, const void* x, int32_t xdt, int64_t ldx, void* y, int32_t ydt, int64_t ldy,
+               int64_t n_cols, void* ws, int64_t ws_bytes, void* stream) {
+  if (!P || op < CBM_OP_AX || op > CBM_OP_DAD_ADD || n_cols < 0) return CBM_ERR_INVALID;
+  if (!dtype_ok(xdt, ydt)) return CBM_ERR_DTYPE;
+  if (n_cols == 0 || P->n_rows == 0) return CBM_OK;
+  if (!x || !y) return CBM_ERR_INVALID;
+  if (ldx < n_cols || ldy < n_cols) return CBM_ERR_SHAPE;
+  if (overlaps(x, P->n_cols * ldx * elem_size(xdt), y, P->n_rows * ldy * elem_size(ydt))) return CBM_ERR_SHAPE;
+  const bool needs_mult = op == CBM_OP_ADX || op == CBM_OP_DADX || op == CBM_OP_VALUES_RATIO || op == CBM_OP_DAD_ADD;
+  if (needs_mult && (!P->d_mult || P->n_rows != P->n_cols)) return CBM_ERR_UNSUPPORTED;
+  if ((op == CBM_OP_VALUES_ADD || op == CBM_OP_VALUES_RATIO) && xdt != CBM_F32) return CBM_ERR_DTYPE;
+  const int64_t need = cbm_plan_workspace_bytes(P, op, n_cols, xdt, ydt, 0);
+  const bool need_ws = P->n_chunks > 0 || (ydt == CBM_BF16 && P->n_internal > 0);
+  if (need_ws && (!ws || ws_bytes < need)) return CBM_ERR_WORKSPACE;
+  if (ws && reinterpret_cast<uintptr_t>(ws) % 16 != 0) return CBM_ERR_INVALID;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+
+  int scale = SCALE_SIGN, prop = PROP_ADD;
+  switch (op) {
+    case CBM_OP_AX: break;
+    case CBM_OP_ADX: scale = SCALE_DCOL; break;
+    case CBM_OP_DADX: scale = SCALE_DCOL_DROW; prop = PROP_RATIO; break;
+    case CBM_OP_VALUES_ADD: scale = P->unit_values ? SCALE_SIGN : SCALE_VALUES; break;
+    case CBM_OP_VALUES_RATIO:
+      scale = P->unit_values ? SCALE_SIGN : SCALE_VALUES;
+      prop = PROP_RATIO;
+      break;
+    case CBM_OP_DAD_ADD: scale = SCALE_DCOL_DROW; break;
+  }
+  const Shape sh = pick_shape(xdt, ydt, x, ldx, y, ldy, n_cols);
+  for (int64_t c0 = 0; c0 < n_cols; c0 += sh.cb) {
+    const int64_t cols = std::min(sh.cb, n_cols - c0);
+    const int64_t nvec = cols / sh.v;
+    int team, vpl;
+    team_for(nvec, &team, &vpl);
+    const int64_t ldp = round4(cols);
+    FwdArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.n_items = (int32_t)P->n_items;
+    a.node = P->d_node;
+    a.ptr = P->d_ptr;
+    a.ent = P->d_ent;
+    a.val = P->d_val;
+    a.par = P->d_par;
+    a.self_slot = P->d_self_slot;
+    a.par_slot = P->d_par_slot;
+    a.chunk0 = P->d_chunk0;
+    a.n_chunks = (int32_t)P->n_chunks;
+    a.chunk_item = P->d_chunk_item;
+    a.chunk_beg = P->d_chunk_beg;
+    a.chunk_end = P->d_chunk_end;
+    a.mult = P->d_mult;
+    a.node_flag = P->d_node_flag;
+    a.chunk_flag = P->d_chunk_flag;
+    a.qs = P->d_qs;
+    a.x = static_cast<const char*>(x) + c0 * elem_size(xdt);
+    a.ldx = ldx;
+    a.y = static_cast<char*>(y) + c0 * elem_size(ydt);
+    a.ldy = ldy;
+    a.nvec = (int32_t)nvec;
+    a.ldp = (int32_t)ldp;
+    a.partial = static_cast<float*>(ws);
+    a.pstate = ws ? static_cast<float*>(ws) + P->n_chunks * ldp : nullptr;
+    a.scale_mode = scale;
+    a.prop_mode = prop;
+    a.team = team;
+    a.rows_per_claim = P->rows_per_claim;
+    a.timeout_ns = P->timeout_ns;
+    const int rc = launch_fwd(P, a, xdt, ydt, sh.vec, vpl, st);
+    if (rc) return rc;
+  }
+  return CBM_OK;
+}
+
+int cbm_plan_prepare_adjoint(cbm_plan* P, void* stream) {
+  if (!P) return CBM_ERR_INVALID;
+  return build_adjoint(P, static_cast<cudaStream_t>(stream));
+}
+
+int cbm_matmul_adjoint(cbm_plan* P, int32_t op, const void* g, int32_t gdt, int64_t ldg, void* dx, int32_t ddt,
+                       int64_t lddx, int64_t n_cols, void* ws, int64_t ws_bytes, void* stream) {
+  if (!P || op < CBM_OP_AX || op > CBM_OP_DADX || n_cols < 0) return CBM_ERR_INVALID;
+  if (!dtype_ok(gdt, ddt)) return CBM_ERR_DTYPE;
+  if (n_cols == 0 || P->n_rows == 0 || P->n_cols == 0) return CBM_OK;
+  if (!g || !dx) return CBM_ERR_INVALID;
+  if (ldg < n_cols || lddx < n_cols) return CBM_ERR_SHAPE;
+  if (overlaps(g, P->n_rows * ldg * elem_size(gdt), dx, P->n_cols * lddx * elem_size(ddt))) return CBM_ERR_SHAPE;
+  if ((op == CBM_OP_ADX || op == CBM_OP_DADX) && (!P->d_mult || P->n_rows != P->n_cols)) return CBM_ERR_UNSUPPORTED;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int rc = build_adjoint(P, st);
+  if (rc) return rc;
+  const int64_t need = cbm_plan_workspace_bytes(P, op, n_cols, gdt, ddt, 1);
+  const bool need_ws = P->n_internal > 0 || P->n_t_chunks > 0;
+  if (need_ws && (!ws || ws_bytes < need)) return CBM_ERR_WORKSPACE;
+  if (ws && reinterpret_cast<uintptr_t>(ws) % 16 != 0) return CBM_ERR_INVALID;
+  const Shape sh = pick_shape(gdt, ddt, g, ldg, dx, lddx, n_cols);
+  for (int64_t c0 = 0; c0 < n_cols; c0 += sh.cb) {
+    const int64_t cols = std::min(sh.cb, n_cols - c0);
+    const int64_t nvec = cols / sh.v;
+    int team, vpl;
+    team_for(nvec, &team, &vpl);
+    const int64_t ldp = round4(cols);
+    float* h = static_cast<float*>(ws);
+    float* partial = ws ? h + P->n_internal * ldp : nullptr;
+    const void* gb = static_cast<const char*>(g) + c0 * elem_size(gdt);
+    if (P->n_internal > 0) {
+      RevArgs r;
+      std::memset(&r, 0, sizeof(r));
+      r.n_items = (int32_t)P->n_internal;
+      r.node = P->d_rev_node;
+      r.slot = P->d_rev_slot;
+      r.ptr = P->d_rev_ptr;
+      r.ent = P->d_rev_ent;
+      r.mult = P->d_mult;
+      r.scale_g = op == CBM_OP_DADX;
+      r.flag = P->d_adj_flag;
+      r.qs = P->d_qs;
+      r.g = gb;
+      r.ldg = ldg;
+      r.h = h;
+      r.ldp = (int32_t)ldp;
+      r.nvec = (int32_t)nvec;
+      r.team = team;
+      r.rows_per_claim = P->rows_per_claim;
+      r.timeout_ns = P->timeout_ns;
+      if ((rc = launch_rev(P, r, gdt, sh.vec, vpl, st))) return rc;
+    }
+    TrArgs t;
+    std::memset(&t, 0, sizeof(t));
+    t.n_items = (int32_t)P->n_cols;
+    t.ptr = P->d_t_ptr;
+    t.ent = P->d_t_ent;
+    t.n_chunks = (int32_t)P->n_t_chunks;
+    t.chunk0 = P->d_t_chunk0;
+    t.chunk_item = P->d_t_chunk_item;
+    t.chunk_beg = P->d_t_chunk_beg;
+    t.chunk_end = P->d_t_chunk_end;
+    t.chunk_flag = P->d_t_chunk_flag;
+    t.mult = P->d_mult;
+    t.scale_g = op == CBM_OP_DADX;
+    t.scale_out = op == CBM_OP_ADX || op == CBM_OP_DADX;
+    t.qs = P->d_qs;
+    t.g = gb;
+    t.ldg = ldg;
+    t.h = h;
+    t.ldp = (int32_t)ldp;
+    t.dx = static_cast<char*>(dx) + c0 * elem_size(ddt);
+    t.lddx = lddx;
+    t.nvec = (int32_t)nvec;
+    t.partial = partial;
+    t.team = team;
+    t.rows_per_claim = P->rows_per_claim;
+    t.timeout_ns = P->timeout_ns;
+    if ((rc = launch_tr(P, t, gdt, ddt, sh.vec, vpl, st))) return rc;
+  }
+  return CBM_OK;
+}
+
+}  // extern "C"

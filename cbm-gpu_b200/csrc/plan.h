@@ -1,0 +1,74 @@
+// The plan object behind the opaque cbm_plan handle (include/cbm_b200.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "kernels.cuh"
+
+struct cbm_plan {
+  int device = 0;
+  int64_t n_rows = 0, n_cols = 0, nnz = 0, n_edges = 0, n_branches = 0;
+  int64_t n_items = 0, n_internal = 0, levels = 0;
+  bool unit_values = true, has_values = false;
+  int32_t chunk_nnz = 256;      // split rows longer than this
+  int32_t rows_per_claim = 4;   // rows a team takes per queue claim
+  int64_t launches = 0;
+  int64_t last_grid = 0;
+  long long timeout_ns = 1000000000ll;  // bounded waits: 1 s
+
+  // host copies used to rebuild chunk tables and the adjoint layout
+  std::vector<int64_t> h_ptr;     // entry offsets per item (level order)
+  std::vector<int32_t> h_order;   // node of each item
+  std::vector<int32_t> h_parent;  // parent per node (-1: virtual root)
+  std::vector<int32_t> h_slot;    // internal slot per node (-1: leaf)
+  std::vector<int32_t> h_depth;
+  std::vector<uint32_t> h_ent;    // column | sign << 31, item order
+
+  // forward layout (device)
+  int32_t* d_node = nullptr;
+  int64_t* d_ptr = nullptr;
+  uint32_t* d_ent = nullptr;
+  float* d_val = nullptr;
+  int32_t* d_par = nullptr;
+  int32_t* d_self_slot = nullptr;
+  int32_t* d_par_slot = nullptr;
+  float* d_mult = nullptr;
+  unsigned* d_node_flag = nullptr;
+  cbm::QueueState* d_qs = nullptr;
+  // forward chunks
+  int64_t n_chunks = 0, long_rows = 0;
+  int32_t* d_chunk0 = nullptr;
+  int32_t* d_chunk_item = nullptr;
+  int64_t* d_chunk_beg = nullptr;
+  int64_t* d_chunk_end = nullptr;
+  unsigned* d_chunk_flag = nullptr;
+
+  // adjoint layout (built on first use)
+  bool adj_built = false;
+  int32_t* d_rev_node = nullptr;   // internal nodes, deepest level first
+  int32_t* d_rev_slot = nullptr;
+  int64_t* d_rev_ptr = nullptr;    // children lists
+  uint32_t* d_rev_ent = nullptr;   // child | internal << 30 (slot if internal)
+  unsigned* d_adj_flag = nullptr;  // [n_internal]
+  std::vector<int64_t> h_t_ptr;    // transposed delta: entries per column
+  int64_t* d_t_ptr = nullptr;
+  uint32_t* d_t_ent = nullptr;     // row (or slot) | internal << 30 | sign << 31
+  int64_t n_t_chunks = 0;
+  int32_t* d_t_chunk0 = nullptr;
+  int32_t* d_t_chunk_item = nullptr;
+  int64_t* d_t_chunk_beg = nullptr;
+  int64_t* d_t_chunk_end = nullptr;
+  unsigned* d_t_chunk_flag = nullptr;
+
+  std::vector<void*> bufs, chunk_bufs, adj_bufs, adj_chunk_bufs;
+};
+
+namespace cbm {
+int cuda_status(cudaError_t e);
+void free_all(std::vector<void*>& v);
+int build_chunks(cbm_plan* P, cudaStream_t st);
+int rebuild_adjoint_chunks(cbm_plan* P, cudaStream_t st);
+}  // namespace cbm

@@ -1,0 +1,195 @@
+/*
+ * cbm_b200.h - C ABI of the B200 CBM (Compressed Binary Matrix) library.
+ *
+ * A binary adjacency matrix A (N x N) is stored as
+ *   - a delta matrix D (CSR, values +-1): row v = A[v] - A[parent(v)], or A[v]
+ *     when v hangs from the virtual root;
+ *   - a compression tree (a forest over the rows) given as branch offsets and
+ *     (parent, child) edges in BFS order per branch.
+ * The product is Y = D*X followed by Y[v] += Y[parent(v)] from the roots down.
+ *
+ * Every function returns CBM_OK (0) or a status code; cbm_status_string()
+ * names it.  No function takes or returns framework (torch) types: pointers are
+ * plain host or device addresses, sizes are element counts, and `stream` is a
+ * cudaStream_t passed as void*.
+ *
+ * Reference interfaces replaced (paths within cbm4scale/CBM-GPU):
+ *   cbm_build / cbm_structure_*       cbm_init_                cbm/cbm_extensions.cpp:60-345
+ *   cbm_plan_create                   cusparseCBM::cusparseCBM cbm/cbm.cu:95-142
+ *   cbm_plan_destroy                  cusparseCBM::~cusparseCBM cbm/cbm.cu:144-147
+ *   cbm_matmul(CBM_OP_VALUES_ADD)     cusparseCBM::matmul_AX_ADX   cbm/cbm.cu:150-207
+ *   cbm_matmul(CBM_OP_VALUES_RATIO)   cusparseCBM::matmul_DAX_DADX cbm/cbm.cu:210-268
+ *   cbm_matmul(CBM_OP_AX/ADX/DADX)    cbm4mm.matmul / cbm4ad.matmul / cbm4dad.matmul
+ *                                     (cbm/cbm4mm.py:53-54, cbm/cbm4ad.py via cbm4mm,
+ *                                      cbm/cbm4dad.py:53-54) with the D^-1/2 scaling
+ *                                     applied on the fly instead of pre-scaled values
+ *                                     (cbm/cbm4ad.py:19-25, cbm/cbm4dad.py:19-34)
+ *   cbm_matmul_adjoint                no counterpart: A^T*G in CBM form (autograd)
+ */
+#ifndef CBM_B200_H
+#define CBM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+  CBM_OK = 0,
+  CBM_ERR_INVALID = 1,     /* null pointer, negative size, bad enum */
+  CBM_ERR_INDEX = 2,       /* an index outside [0, n) */
+  CBM_ERR_ALLOC = 3,       /* host or device allocation failed */
+  CBM_ERR_CUDA = 4,        /* a CUDA runtime call failed */
+  CBM_ERR_STRUCTURE = 5,   /* not a forest / duplicate child / bad offsets */
+  CBM_ERR_DTYPE = 6,       /* unsupported dtype combination */
+  CBM_ERR_SHAPE = 7,       /* leading dimension < columns, aliasing x and y */
+  CBM_ERR_TIMEOUT = 8,     /* a device wait ran out (see cbm_plan_error) */
+  CBM_ERR_UNSUPPORTED = 9, /* op needs multipliers / values the plan lacks */
+  CBM_ERR_WORKSPACE = 10,  /* workspace smaller than cbm_plan_workspace_bytes */
+  CBM_ERR_INTERNAL = 11
+};
+
+/* ---- dtypes and ops ------------------------------------------------------ */
+enum { CBM_F32 = 0, CBM_BF16 = 1 };
+
+enum {
+  CBM_OP_AX = 0,          /* Y = A X             (signs only)                     */
+  CBM_OP_ADX = 1,         /* Y = A D^-1/2 X      (signs, D[col] on the fly)       */
+  CBM_OP_DADX = 2,        /* Y = D^-1/2 A D^-1/2 X (signs, D[col]*D[row], ratio)  */
+  CBM_OP_VALUES_ADD = 3,  /* Y = Dv X; Y[v] += Y[u]            (matmul_AX_ADX)   */
+  CBM_OP_VALUES_RATIO = 4, /* Y = Dv X; Y[v] += Y[u]*m[v]/m[u]  (matmul_DAX_DADX) */
+  CBM_OP_DAD_ADD = 5       /* entries s*m[col]*m[row], Y[v] += Y[u]: what matmul_AX_ADX
+                              computes on the values cbm4dad prepares                 */
+};
+
+/* ---- construction (host, OpenMP) ----------------------------------------- */
+typedef struct cbm_structure cbm_structure;
+
+enum { CBM_BUILD_EXHAUSTIVE = 1 }; /* every pair sharing a column (for checks) */
+
+/* Builds delta matrix + tree from COO (row, col) of a binary N x N matrix.
+ * Replaces cbm_init_ (cbm/cbm_extensions.cpp:60-345). n_threads <= 0: all. */
+int cbm_build(const int32_t* row, const int32_t* col, int64_t nnz, int64_t n_rows, int64_t alpha,
+              int32_t n_threads, int32_t flags, cbm_structure** out);
+
+/* The six arrays cbm_init_ returns (cbm/cbm_extensions.cpp:301-344), in its
+ * order, then extras: the delta matrix as CSR (rows sorted, one block per row),
+ * the parent of each node (N = virtual root), and counters. */
+enum {
+  CBM_S_DELTA_ROW = 0, /* int32 [Z]   child id of each delta entry            */
+  CBM_S_DELTA_COL = 1, /* int32 [Z]                                           */
+  CBM_S_DELTA_VAL = 2, /* float [Z]   +-1                                     */
+  CBM_S_BRANCHES = 3,  /* int32 [B+1] prefix sums of edges per branch         */
+  CBM_S_SRC = 4,       /* int32 [E]   parent of each tree edge (BFS order)    */
+  CBM_S_DST = 5,       /* int32 [E]   child  of each tree edge                */
+  CBM_S_PARENT = 6,    /* int32 [N]                                           */
+  CBM_S_CSR_PTR = 7,   /* int32 [N+1]                                         */
+  CBM_S_CSR_COL = 8,   /* int32 [Z]                                           */
+  CBM_S_CSR_VAL = 9,   /* float [Z]                                           */
+  CBM_S_N_CANDIDATES = 100, /* length-only queries */
+  CBM_S_TREE_COST = 101,
+  CBM_S_NNZ_A = 102
+};
+int64_t cbm_structure_len(const cbm_structure* s, int32_t which);
+int cbm_structure_copy(const cbm_structure* s, int32_t which, void* dst);
+void cbm_structure_free(cbm_structure* s);
+
+/* Host-only check of a delta matrix + tree (CSR row pointers monotone and
+ * ending at nnz, columns in range, branch offsets a prefix sum ending at
+ * n_edges, parents/children in range, no node with two parents, no cycle).
+ * cbm_plan_create runs the same checks.  Host pointers. */
+int cbm_validate(const int32_t* row_ptr, const int32_t* col_idx, int64_t n_rows, int64_t n_cols, int64_t nnz,
+                 const int32_t* branches, int64_t n_branch_offsets, const int32_t* src, const int32_t* dst,
+                 int64_t n_edges);
+
+/* ---- device plan ----------------------------------------------------------- */
+typedef struct cbm_plan cbm_plan;
+
+enum {
+  CBM_INPUT_DEVICE = 0, /* structure pointers are device addresses */
+  CBM_INPUT_HOST = 1    /* structure pointers are host addresses   */
+};
+
+/* Uploads the structure in the kernels' layout (rows in tree-level order,
+ * column index and sign packed in one word, long rows split in chunks).
+ * values (nnz floats) give each entry's sign and, for the VALUES ops, its
+ * value; NULL means every entry is +1.  multipliers (N floats, may be NULL)
+ * are copied.
+ * Replaces cusparseCBM::cusparseCBM (cbm/cbm.cu:95-142). */
+int cbm_plan_create(const int32_t* row_ptr, const int32_t* col_idx, const float* values, int64_t n_rows,
+                    int64_t n_cols, int64_t nnz, const int32_t* branches, int64_t n_branch_offsets,
+                    const int32_t* src, const int32_t* dst, int64_t n_edges, const float* multipliers,
+                    int32_t input_kind, void* stream, cbm_plan** out);
+
+/* Copies N multipliers (device pointer) into the plan: D^-1/2 for ADX/DADX. */
+int cbm_plan_set_multipliers(cbm_plan* plan, const float* d_multipliers, void* stream);
+
+/* Re-splits long rows: rows with more than `chunk_nnz` entries are summed in
+ * chunks of that size by separate warps (>= 32). rows_per_claim: rows a team
+ * takes per queue claim (>= 1).  Host-side re-layout + upload. */
+int cbm_plan_tune(cbm_plan* plan, int32_t chunk_nnz, int32_t rows_per_claim, void* stream);
+
+/* Device scratch bytes a call with these operand types needs (0 is possible). */
+int64_t cbm_plan_workspace_bytes(const cbm_plan* plan, int32_t op, int64_t n_cols, int32_t x_dtype,
+                                 int32_t y_dtype, int32_t adjoint);
+
+/* Y = op(A) X.  x: [n_rows, n_cols] row-major with leading dimension ldx, y
+ * likewise with ldy; both device memory, not overlapping.  workspace: device
+ * scratch of at least cbm_plan_workspace_bytes() bytes.  Allocates nothing,
+ * launches one kernel on `stream`, does not synchronise. Calls on one plan must
+ * be ordered (one stream, or events): they share the plan's queue state.
+ * Replaces matmul_AX_ADX / matmul_DAX_DADX (cbm/cbm.cu:150-268). */
+int cbm_matmul(cbm_plan* plan, int32_t op, const void* x, int32_t x_dtype, int64_t ldx, void* y,
+               int32_t y_dtype, int64_t ldy, int64_t n_cols, void* workspace, int64_t workspace_bytes,
+               void* stream);
+
+/* dX = op(A)^T G (the adjoint of cbm_matmul for CBM_OP_AX/ADX/DADX): a
+ * reverse tree propagation (children into parents) then a transposed delta
+ * gather.  Same conventions as cbm_matmul.  No counterpart in the reference. */
+int cbm_matmul_adjoint(cbm_plan* plan, int32_t op, const void* g, int32_t g_dtype, int64_t ldg, void* dx,
+                       int32_t dx_dtype, int64_t lddx, int64_t n_cols, void* workspace,
+                       int64_t workspace_bytes, void* stream);
+
+/* Builds the adjoint layout (reverse-propagation lists and the transposed
+ * delta matrix) ahead of the first cbm_matmul_adjoint; synchronous. */
+int cbm_plan_prepare_adjoint(cbm_plan* plan, void* stream);
+
+/* Limit of every device-side wait, in nanoseconds (default 1 s). */
+int cbm_plan_set_timeout(cbm_plan* plan, int64_t ns);
+
+/* Test hook: make queue item `item` wait on `parent_node` (whose ready flag may
+ * never be set) to exercise the bounded wait.  -1 removes the parent. */
+int cbm_plan_debug_set_parent(cbm_plan* plan, int64_t item, int32_t parent_node, void* stream);
+
+/* Synchronises `stream`, returns the first device-side error recorded since
+ * the last call (CBM_OK, CBM_ERR_TIMEOUT, CBM_ERR_INDEX) in *device_status and
+ * clears it. info (may be NULL) receives where it happened. */
+int cbm_plan_error(cbm_plan* plan, void* stream, int32_t* device_status, int64_t* info);
+
+/* Plan statistics (for the bench's algorithmic byte counts). */
+enum {
+  CBM_P_ROWS = 0,
+  CBM_P_COLS = 1,
+  CBM_P_NNZ = 2,
+  CBM_P_EDGES = 3,
+  CBM_P_BRANCHES = 4,
+  CBM_P_LEVELS = 5,
+  CBM_P_INTERNAL = 6,
+  CBM_P_CHUNKS = 7,
+  CBM_P_LONG_ROWS = 8,
+  CBM_P_UNIT_VALUES = 9,
+  CBM_P_GRID = 10,
+  CBM_P_LAUNCHES = 11 /* kernels launched by this plan so far */
+};
+int64_t cbm_plan_stat(const cbm_plan* plan, int32_t which);
+
+void cbm_plan_destroy(cbm_plan* plan);
+
+const char* cbm_status_string(int32_t status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CBM_B200_H */

@@ -1,0 +1,279 @@
+"""GPU parity of the forward products against the oracle (CPU restatement of
+the reference's products, cbm/cbm.cu:150-268 and cbm/cbm_extensions.cpp:351-698).
+
+Rows that are not split into chunks are summed in the same order as the
+oracle (sequential FMAs over the row's entries) and the propagation uses the
+reference's arithmetic, so those results must be bit-identical.  Split rows
+are summed chunk by chunk: rtol 1e-5, atol 1e-6 (the reference's own
+tolerance, scripts/validate.sh:12-13, plus an absolute floor).
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import chain_graph, near_dup_graph, random_graph
+
+pytestmark = pytest.mark.gpu
+
+RTOL, ATOL = 1e-5, 1e-6
+
+
+def _dev():
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    return torch.device("cuda")
+
+
+def _make(cls_name, ei, alpha=0):
+    from cbm import cbm4ad, cbm4dad, cbm4mm
+
+    cls = {"ax": cbm4mm.cbm4mm, "adx": cbm4ad.cbm4ad, "dadx": cbm4dad.cbm4dad}[cls_name]
+    return cls(torch.from_numpy(ei), torch.ones(ei.shape[1]), alpha=alpha)
+
+
+def _oracle(op, a, x):
+    from oracle import oracle
+
+    crow = a.deltas.crow_indices().cpu().numpy()
+    col = a.deltas.col_indices().cpu().numpy()
+    val = a.deltas.values().cpu().numpy()  # the reference's prepared values
+    br = a.mca_offset.cpu().numpy()
+    src = a.mca_src_idx.cpu().numpy()
+    dst = a.mca_dst_idx.cpu().numpy()
+    xn = x.float().cpu().numpy()
+    if op == "dadx":
+        return oracle.spmm_fused_update(crow, col, val, xn, br, src, dst, a.D.cpu().numpy(), gpu_order=True)
+    return oracle.spmm_update(crow, col, val, xn, br, src, dst)
+
+
+def _f64(op, ei, n, x):
+    from oracle import oracle
+
+    ptr, idx = oracle.csr_from_edges(ei, n)
+    d = np.diff(ptr).astype(np.float64)
+    with np.errstate(divide="ignore"):
+        dinv = 1.0 / np.sqrt(d)
+    rs = dinv if op == "dadx" else None
+    cs = dinv if op in ("adx", "dadx") else None
+    return oracle.dense_f64(ptr, idx, n, x.double().cpu().numpy(), rs=rs, cs=cs)
+
+
+GRAPHS = {
+    "near_dup": lambda: (near_dup_graph(3000, seed=11, deg=14), 3000),
+    "random": lambda: (random_graph(2000, 9, seed=4), 2000),
+    "community": lambda: (__import__("cbm.synthetic", fromlist=["x"]).workload("community-4096")[0], 4096),
+}
+
+
+@pytest.mark.parametrize("graph", list(GRAPHS))
+@pytest.mark.parametrize("op", ["ax", "adx", "dadx"])
+@pytest.mark.parametrize("cols", [64, 256])
+def test_forward_bit_exact_vs_oracle(graph, op, cols):
+    dev = _dev()
+    ei, n = GRAPHS[graph]()
+    a = _make(op, ei, alpha=0)
+    assert a.plan.stat(7) == 0, "no row should be split at these sizes"
+    g = torch.Generator(device="cpu").manual_seed(0)
+    x = (torch.rand(n, cols, generator=g) * 2 - 1).to(dev)
+    y = torch.empty(n, cols, device=dev)
+    a.matmul(x, y)
+    torch.cuda.synchronize()
+    ref = _oracle(op, a, x)
+    np.testing.assert_array_equal(y.cpu().numpy(), ref)
+    # and close to the exact product
+    y64 = _f64(op, ei, n, x)
+    err = np.abs(y.cpu().numpy() - y64).max()
+    assert err < 1e-4 * max(1.0, np.abs(y64).max())
+    a.plan.check_device()
+
+
+@pytest.mark.parametrize("op", ["ax", "dadx"])
+def test_split_rows(op):
+    """Force chunking (rows longer than 32 entries) and compare to the oracle."""
+    dev = _dev()
+    from cbm.synthetic import chung_lu_graph, near_duplicates
+
+    rng = np.random.Generator(np.random.PCG64(3))
+    ei = near_duplicates(chung_lu_graph(5000, 2.1, 20.0, rng=rng), 5000, 0.3, 0.1, rng=rng)
+    a = _make(op, ei, alpha=0)
+    a.plan.tune(chunk_nnz=32, rows_per_claim=2)
+    st = a.plan.stats
+    assert st["chunks"] > 0 and st["long_rows"] > 0
+    x = torch.randn(5000, 128, device=dev)
+    y = torch.empty_like(x)
+    a.matmul(x, y)
+    ref = _oracle(op, a, x)
+    torch.testing.assert_close(y.cpu(), torch.from_numpy(ref), rtol=RTOL, atol=ATOL)
+    a.plan.check_device()
+
+
+def test_deep_chain():
+    """A 600-deep chain: every row waits on its parent."""
+    dev = _dev()
+    ei, n = chain_graph(600)
+    a = _make("ax", ei)
+    assert a.plan.stats["levels"] == 600
+    x = torch.randn(n, 32, device=dev)
+    y = torch.empty_like(x)
+    a.matmul(x, y)
+    np.testing.assert_array_equal(y.cpu().numpy(), _oracle("ax", a, x))
+    a.plan.check_device()
+
+
+@pytest.mark.parametrize("cols", [1, 3, 40, 1100])
+def test_column_counts(cols):
+    """Scalar path (odd widths), partial teams and the column split beyond 1024."""
+    dev = _dev()
+    ei = near_dup_graph(1500, seed=2)
+    a = _make("dadx", ei)
+    x = torch.randn(1500, cols, device=dev)
+    y = torch.empty_like(x)
+    a.matmul(x, y)
+    np.testing.assert_array_equal(y.cpu().numpy(), _oracle("dadx", a, x))
+
+
+def test_strided_and_misaligned_views():
+    dev = _dev()
+    ei = near_dup_graph(1200, seed=6)
+    a = _make("ax", ei)
+    big = torch.randn(1200, 136, device=dev)
+    out = torch.zeros(1200, 136, device=dev)
+    # leading dimension 136, 64 columns, 16-byte aligned: vector path
+    a.matmul(big[:, :64], out[:, :64])
+    np.testing.assert_array_equal(out[:, :64].cpu().numpy(), _oracle("ax", a, big[:, :64].contiguous()))
+    assert torch.all(out[:, 64:] == 0)
+    # offset by one column: scalar path
+    a.matmul(big[:, 1:65], out[:, 1:65])
+    np.testing.assert_array_equal(out[:, 1:65].cpu().numpy(), _oracle("ax", a, big[:, 1:65].contiguous()))
+
+
+@pytest.mark.parametrize("ydt", [torch.float32, torch.bfloat16])
+def test_bf16_inputs(ydt):
+    """BF16 X, FP32 accumulation: equal to the fp32 oracle on the same (bf16) values."""
+    dev = _dev()
+    ei = near_dup_graph(2500, seed=8)
+    a = _make("dadx", ei)
+    x = torch.randn(2500, 128, device=dev).to(torch.bfloat16)
+    y = torch.empty(2500, 128, device=dev, dtype=ydt)
+    a.matmul(x, y)
+    ref = torch.from_numpy(_oracle("dadx", a, x))
+    assert torch.equal(y.cpu(), ref.to(ydt))
+
+
+def test_dropin_cusparseCBM_reference_preparation():
+    """The reference's own preparation (cbm/cbm4mm.py:26-51, cbm/cbm4dad.py:11-51) fed to cusparseCBM."""
+    dev = _dev()
+    from cbm import cbm_mkl_cpp
+    from cbm.cbm_cusparse import cusparseCBM
+
+    ei = torch.from_numpy(near_dup_graph(2000, seed=3))
+    n = int(max(ei[0].max(), ei[1].max())) + 1
+    data = cbm_mkl_cpp.init(ei[0], ei[1], torch.ones(ei.shape[1]), n, 0)
+    deltas = torch.sparse_coo_tensor(torch.stack([data[0], data[1]]).to(torch.int32), data[2],
+                                     (n, n)).coalesce().to_sparse_csr()
+    deltas = torch.sparse_csr_tensor(deltas.crow_indices().to(torch.int32), deltas.col_indices().to(torch.int32),
+                                     deltas.values().to(torch.float32), deltas.shape).to(dev)
+    br, src, dst = (t.to(dtype=torch.int32, device=dev) for t in data[3:])
+    ext = cusparseCBM(deltas, br, src, dst, torch.empty(0, device=dev))
+    d = torch.zeros(n, 1, device=dev)
+    assert ext.matmul_AX_ADX(torch.ones(n, 1, device=dev), d) == 0
+    D = (d ** (-1 / 2)).view(-1)
+    vals = deltas.values() * D[deltas.col_indices()]
+    rows = torch.repeat_interleave(torch.arange(n, device=dev), torch.diff(deltas.crow_indices()))
+    vals = vals * D[rows]
+    dad = torch.sparse_csr_tensor(deltas.crow_indices(), deltas.col_indices(), vals, deltas.shape)
+    ext2 = cusparseCBM(dad, br, src, dst, D)
+    x = torch.rand(n, 96, device=dev)
+    y = torch.empty_like(x)
+    assert ext2.matmul_DAX_DADX(x, y) == 0
+    from oracle import oracle
+
+    ref = oracle.spmm_fused_update(dad.crow_indices().cpu().numpy(), dad.col_indices().cpu().numpy(),
+                                   vals.cpu().numpy(), x.cpu().numpy(), br.cpu().numpy(), src.cpu().numpy(),
+                                   dst.cpu().numpy(), D.cpu().numpy())
+    np.testing.assert_array_equal(y.cpu().numpy(), ref)
+    with pytest.raises(RuntimeError):
+        ext.matmul_DAX_DADX(x, y)
+
+
+def test_isolated_nodes_dad():
+    dev = _dev()
+    ei = random_graph(800, 6, seed=1, isolated=50)
+    a = _make("dadx", ei)
+    assert torch.isinf(a.D).sum() >= 50
+    x = torch.randn(800, 64, device=dev)
+    y = torch.empty_like(x)
+    a.matmul(x, y)
+    out = y.cpu().numpy()
+    np.testing.assert_array_equal(out, _oracle("dadx", a, x))
+    assert np.all(out[750:] == 0)
+
+
+def test_operand_errors():
+    dev = _dev()
+    a = _make("ax", near_dup_graph(300, seed=1))
+    x = torch.randn(300, 16, device=dev)
+    y = torch.empty(300, 16, device=dev)
+    with pytest.raises(RuntimeError):
+        a.matmul(x.cpu(), y)
+    with pytest.raises(RuntimeError):
+        a.matmul(x.double(), y)
+    with pytest.raises(RuntimeError):
+        a.matmul(x[:200], y[:200])
+    with pytest.raises(RuntimeError):
+        a.matmul(x, torch.empty(300, 8, device=dev))
+    with pytest.raises(RuntimeError):
+        a.matmul(x, x)  # aliasing
+    with pytest.raises(RuntimeError):
+        a.matmul(x.to(torch.float32), y.to(torch.bfloat16))  # fp32 -> bf16 is not a supported pair
+
+
+def test_repeatable_and_graph_capturable():
+    dev = _dev()
+    a = _make("dadx", near_dup_graph(3000, seed=12))
+    x = torch.randn(3000, 64, device=dev)
+    y1 = torch.empty_like(x)
+    y2 = torch.empty_like(x)
+    a.matmul(x, y1)
+    a.matmul(x, y2)
+    assert torch.equal(y1, y2)
+    # capture in a CUDA graph and replay on new inputs
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        a.matmul(x, y2)
+    torch.cuda.current_stream().wait_stream(s)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        a.matmul(x, y2)
+    for seed in range(3):
+        x.copy_(torch.randn(3000, 64, device=dev, generator=torch.Generator(device=dev).manual_seed(seed)))
+        graph.replay()
+        a.matmul(x, y1)
+        torch.cuda.synchronize()
+        assert torch.equal(y1, y2)
+    a.plan.check_device()
+
+
+def test_bounded_wait_times_out_and_recovers():
+    """A row made to wait on a flag that nothing sets: the kernel returns, the
+    status says timeout, and the plan keeps working."""
+    dev = _dev()
+    from cbm import _lib
+
+    a = _make("ax", near_dup_graph(500, seed=4))
+    p = a.plan
+    has_child = set(a.mca_src_idx.cpu().tolist())
+    leaf = next(v for v in range(500) if v not in has_child)
+    p.set_timeout(5_000_000)  # 5 ms
+    rc = p._lib.cbm_plan_debug_set_parent(p._h, 0, leaf, None)
+    assert rc == 0
+    x = torch.randn(500, 32, device=dev)
+    y = torch.empty_like(x)
+    a.matmul(x, y)
+    st, info = p.error()
+    assert st == _lib.ERR_TIMEOUT
+    assert p._lib.cbm_plan_debug_set_parent(p._h, 0, -1, None) == 0
+    p.set_timeout(1_000_000_000)
+    a.matmul(x, y)
+    assert p.error()[0] == _lib.OK
+    np.testing.assert_array_equal(y.cpu().numpy(), _oracle("ax", a, x))
