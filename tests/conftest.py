@@ -27,9 +27,12 @@ def random_graph(n, avg_deg, seed, symmetric=True, self_loops=False, isolated=0)
 
     rng = np.random.Generator(np.random.PCG64(seed))
     m = int(n * avg_deg / (2 if symmetric else 1))
-    active = n - isolated
-    r = rng.integers(0, active, m)
-    c = rng.integers(0, active, m)
+    # isolated nodes are ids [n//4, n//4 + isolated): inside the index range
+    active_ids = np.setdiff1d(np.arange(n), np.arange(n // 4, n // 4 + isolated))
+    active = active_ids.size
+    r = active_ids[rng.integers(0, active, m)]
+    c = active_ids[rng.integers(0, active, m)]
+    r[0], c[0] = 0, n - 1  # both ends present, so that max(index) + 1 == n
     if symmetric:
         ei = coalesce_symmetric(r, c, n)
     else:
@@ -37,7 +40,7 @@ def random_graph(n, avg_deg, seed, symmetric=True, self_loops=False, isolated=0)
         key = np.unique(r[keep].astype(np.int64) * n + c[keep])
         ei = np.stack([key // n, key % n]).astype(np.int32)
     if self_loops and symmetric:
-        extra = np.arange(0, active, 3)
+        extra = active_ids[::3]
         key = np.unique(np.concatenate([ei[0].astype(np.int64) * n + ei[1], extra * n + extra]))
         ei = np.stack([key // n, key % n]).astype(np.int32)
     return ei

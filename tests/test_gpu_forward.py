@@ -4,8 +4,9 @@ the reference's products, cbm/cbm.cu:150-268 and cbm/cbm_extensions.cpp:351-698)
 Rows that are not split into chunks are summed in the same order as the
 oracle (sequential FMAs over the row's entries) and the propagation uses the
 reference's arithmetic, so those results must be bit-identical.  Split rows
-are summed chunk by chunk: rtol 1e-5, atol 1e-6 (the reference's own
-tolerance, scripts/validate.sh:12-13, plus an absolute floor).
+are summed chunk by chunk, in another order: there the difference to the
+FP64 product and to the oracle is bounded by 1e-5 * |P||Delta||X| + 1e-6,
+the magnitude of what was summed (plain rtol fails on cancelling entries).
 """
 import numpy as np
 import pytest
@@ -101,9 +102,41 @@ def test_split_rows(op):
     x = torch.randn(5000, 128, device=dev)
     y = torch.empty_like(x)
     a.matmul(x, y)
+    # chunks are summed separately, so the order differs from the oracle's:
+    # bound the difference by the magnitude of what was summed, S = |P||Delta||X|
     ref = _oracle(op, a, x)
-    torch.testing.assert_close(y.cpu(), torch.from_numpy(ref), rtol=RTOL, atol=ATOL)
+    y64 = _f64(op, ei, 5000, x)
+    s = _abs_sum(op, a, x)
+    out = y.cpu().numpy()
+    # a sequential fp32 sum of n terms is within n * 2^-24 * sum|terms| (the
+    # oracle's own error); n = longest row + depth
+    n_terms = int(np.diff(a.deltas.crow_indices().cpu().numpy()).max()) + st["levels"] + 2
+    gamma = max(1e-5, 2.0 * n_terms * 2.0 ** -24)
+    assert np.all(np.abs(out - y64) <= 1e-5 * s + 1e-6)
+    assert np.all(np.abs(out - ref) <= gamma * s + 1e-6)
     a.plan.check_device()
+
+
+def _abs_sum(op, a, x):
+    """|P| |Delta_op| |X| in fp64: what a product in any summation order adds up."""
+    from oracle import oracle
+
+    crow = a.deltas.crow_indices().cpu().numpy()
+    col = a.deltas.col_indices().cpu().numpy()
+    val = np.abs(a.deltas.values().cpu().numpy()).astype(np.float64)
+    xa = np.abs(x.double().cpu().numpy())
+    n = crow.size - 1
+    s = np.zeros((n, xa.shape[1]))
+    rows = np.repeat(np.arange(n), np.diff(crow))
+    np.add.at(s, rows, val[:, None] * xa[col])
+    src, dst = a.mca_src_idx.cpu().numpy(), a.mca_dst_idx.cpu().numpy()
+    ratio = np.ones(src.size)
+    if op == "dadx":
+        dd = a.D.double().cpu().numpy()
+        ratio = dd[dst] / dd[src]
+    for u, v, r in zip(src, dst, ratio):
+        s[v] += s[u] * r
+    return s
 
 
 def test_deep_chain():
@@ -205,7 +238,7 @@ def test_isolated_nodes_dad():
     a.matmul(x, y)
     out = y.cpu().numpy()
     np.testing.assert_array_equal(out, _oracle("dadx", a, x))
-    assert np.all(out[750:] == 0)
+    assert np.all(out[200:250] == 0)  # the isolated rows
 
 
 def test_operand_errors():
