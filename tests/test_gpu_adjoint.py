@@ -26,6 +26,7 @@ def _adj_f64(op, ei, n, g):
     d = np.diff(ptr).astype(np.float64)
     with np.errstate(divide="ignore"):
         dinv = 1.0 / np.sqrt(d)
+    dinv[d == 0] = 0.0  # an empty row's product is 0 (inf * 0 in exact form)
     # (rs A cs)^T g = cs A^T (rs g)
     rs = dinv if op == "dadx" else None
     cs = dinv if op in ("adx", "dadx") else None

@@ -53,6 +53,7 @@ def _f64(op, ei, n, x):
     d = np.diff(ptr).astype(np.float64)
     with np.errstate(divide="ignore"):
         dinv = 1.0 / np.sqrt(d)
+    dinv[d == 0] = 0.0  # an empty row's product is 0 (inf * 0 in exact form)
     rs = dinv if op == "dadx" else None
     cs = dinv if op in ("adx", "dadx") else None
     return oracle.dense_f64(ptr, idx, n, x.double().cpu().numpy(), rs=rs, cs=cs)
@@ -112,8 +113,10 @@ def test_split_rows(op):
     # oracle's own error); n = longest row + depth
     n_terms = int(np.diff(a.deltas.crow_indices().cpu().numpy()).max()) + st["levels"] + 2
     gamma = max(1e-5, 2.0 * n_terms * 2.0 ** -24)
-    assert np.all(np.abs(out - y64) <= 1e-5 * s + 1e-6)
-    assert np.all(np.abs(out - ref) <= gamma * s + 1e-6)
+    over64 = np.abs(out - y64) - (1e-5 * s + 1e-6)
+    assert over64.max() <= 0, (over64.max(), np.unravel_index(over64.argmax(), over64.shape))
+    over = np.abs(out - ref) - (gamma * s + 1e-6)
+    assert over.max() <= 0, (over.max(), np.unravel_index(over.argmax(), over.shape))
     a.plan.check_device()
 
 
