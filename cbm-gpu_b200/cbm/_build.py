@@ -22,7 +22,7 @@ BUILD = os.path.join(PKG_ROOT, "_build")
 LIB = os.path.join(HERE, "libcbm_b200.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["construct.cpp", "plan.cu", "matmul.cu"]
+SOURCES = ["construct.cpp", "plan.cu", "matmul.cu", "noalloc.cu"]
 HEADERS = ["kernels.cuh", "plan.h"]
 
 

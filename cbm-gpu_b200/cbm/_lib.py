@@ -14,7 +14,8 @@ LIB_PATH = os.path.join(HERE, "libcbm_b200.so")
 
 # status codes (include/cbm_b200.h)
 OK, ERR_INVALID, ERR_INDEX, ERR_ALLOC, ERR_CUDA, ERR_STRUCTURE, ERR_DTYPE, ERR_SHAPE, ERR_TIMEOUT, \
-    ERR_UNSUPPORTED, ERR_WORKSPACE, ERR_INTERNAL = range(12)
+    ERR_UNSUPPORTED, ERR_WORKSPACE, ERR_INTERNAL, ERR_TOO_LARGE = range(13)
+NOALLOC_MAX_ROWS = 1048544
 F32, BF16 = 0, 1
 OP_AX, OP_ADX, OP_DADX, OP_VALUES_ADD, OP_VALUES_RATIO, OP_DAD_ADD = range(6)
 INPUT_DEVICE, INPUT_HOST = 0, 1
@@ -47,6 +48,7 @@ SIGNATURES = [
     ("cbm_plan_set_timeout", C.c_int, [vp, i64]),
     ("cbm_plan_debug_set_parent", C.c_int, [vp, i64, i32, vp]),
     ("cbm_plan_error", C.c_int, [vp, vp, C.POINTER(i32), C.POINTER(i64)]),
+    ("cbm_matmul_noalloc", C.c_int, [vp, vp, vp, i64, i64, vp, vp, i64, vp, vp, vp, i64, vp, vp]),
     ("cbm_plan_stat", i64, [vp, i32]),
     ("cbm_plan_destroy", None, [vp]),
     ("cbm_status_string", C.c_char_p, [i32]),

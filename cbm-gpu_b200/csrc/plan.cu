@@ -168,6 +168,7 @@ const char* cbm_status_string(int32_t s) {
     case CBM_ERR_UNSUPPORTED: return "operation needs multipliers or values the plan does not have";
     case CBM_ERR_WORKSPACE: return "workspace too small";
     case CBM_ERR_INTERNAL: return "internal error";
+    case CBM_ERR_TOO_LARGE: return "too many rows for the fixed scratch of cbm_matmul_noalloc";
     default: return "unknown status";
   }
 }

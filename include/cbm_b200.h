@@ -48,7 +48,8 @@ enum {
   CBM_ERR_TIMEOUT = 8,     /* a device wait ran out (see cbm_plan_error) */
   CBM_ERR_UNSUPPORTED = 9, /* op needs multipliers / values the plan lacks */
   CBM_ERR_WORKSPACE = 10,  /* workspace smaller than cbm_plan_workspace_bytes */
-  CBM_ERR_INTERNAL = 11
+  CBM_ERR_INTERNAL = 11,
+  CBM_ERR_TOO_LARGE = 12   /* beyond cbm_matmul_noalloc's fixed scratch (CBM_NOALLOC_MAX_ROWS) */
 };
 
 /* ---- dtypes and ops ------------------------------------------------------ */
@@ -167,6 +168,31 @@ int cbm_plan_debug_set_parent(cbm_plan* plan, int64_t item, int32_t parent_node,
  * the last call (CBM_OK, CBM_ERR_TIMEOUT, CBM_ERR_INDEX) in *device_status and
  * clears it. info (may be NULL) receives where it happened. */
 int cbm_plan_error(cbm_plan* plan, void* stream, int32_t* device_status, int64_t* info);
+
+/* ---- product without allocation ----------------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory (a plugin inside a process whose allocator owns all of the GPU, a
+ * serving loop that must not take cudaMalloc's implicit synchronisation, an
+ * extension point that is only handed buffers): Y = A X computed straight from
+ * the reference's layout in the caller's device buffers, with no plan and no
+ * workspace.  row_ptr/col_idx/values: the delta matrix as CSR (values NULL =
+ * all +1); src/dst: the tree edges in BFS order per branch (the reference's
+ * mca_src_idx / mca_dst_idx); multipliers NULL gives matmul_AX_ADX, non-NULL
+ * matmul_DAX_DADX (cbm/cbm.cu:150-268).  x: [n_cols, n_x_cols] fp32, y:
+ * [n_rows, n_x_cols] fp32, both contiguous.  d_status (device int32, may be
+ * NULL) receives the device-side status when the work ends (CBM_OK,
+ * CBM_ERR_TIMEOUT, CBM_ERR_INDEX).
+ * Scratch: a fixed 8 MiB array inside the library, held on every GPU that
+ * loads it; n_rows above CBM_NOALLOC_MAX_ROWS returns CBM_ERR_TOO_LARGE.
+ * The first call on a device looks up the array's device address (set-up);
+ * make that first call before any stream capture.  Calls share the array:
+ * calls whose kernels overlap on the GPU race.  Allocates nothing; two kernel
+ * launches on `stream`, no synchronisation. */
+#define CBM_NOALLOC_MAX_ROWS 1048544
+int cbm_matmul_noalloc(const int32_t* row_ptr, const int32_t* col_idx, const float* values, int64_t n_rows,
+                       int64_t n_cols, const int32_t* src, const int32_t* dst, int64_t n_edges,
+                       const float* multipliers, const float* x, float* y, int64_t n_x_cols, int32_t* d_status,
+                       void* stream);
 
 /* Plan statistics (for the bench's algorithmic byte counts). */
 enum {

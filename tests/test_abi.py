@@ -33,7 +33,7 @@ def test_python_binding_covers_the_header():
 def test_status_strings(lib):
     from cbm import _lib
 
-    for code in range(12):
+    for code in range(13):
         assert _lib.status_string(code)
     assert "timed out" in _lib.status_string(_lib.ERR_TIMEOUT)
 
