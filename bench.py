@@ -206,6 +206,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--variant", default="auto", choices=["auto", "register", "staged"])
+    ap.add_argument("--chunk-nnz", type=int, default=256)
+    ap.add_argument("--rows-per-claim", type=int, default=4)
+    ap.add_argument("--team", type=int, default=0)
+    ap.add_argument("--hot-rows", type=int, default=65536)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -231,6 +236,8 @@ def main():
     torch.cuda.set_device(dev)
     ei, n, spec = load_graph(rank, world)
     a = cbm4dad(torch.from_numpy(ei), torch.ones(ei.shape[1]), alpha=spec["alpha"])
+    a.plan.tune(chunk_nnz=args.chunk_nnz, rows_per_claim=args.rows_per_claim, variant=args.variant,
+                hot_rows=args.hot_rows, team=args.team)
     st = a.plan.stats
     z, e, b = st["nnz"], st["edges"], st["branches"]
     b_alg = bytes_alg(n, z, e, b, COLS)
@@ -312,13 +319,15 @@ def main():
             "rows_per_s": n * world / (ms_max * 1e-3),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic_from_profile(),
-                         "kernel": "cbm::fwd_kernel<float,float,2,4>", "bytes_alg_per_launch": b_alg},
+                         "kernel": ("cbm::fwd_kernel<float,float,2,4>" if args.variant == "register"
+                                    else "cbm::fwd_stream_kernel<float,float,2,4,8>"),
+                         "bytes_alg_per_launch": b_alg},
             "e2e": {"value": b_alg * world / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s",
                     "h2d_bytes_per_step": int(xh.numel() * 4), "d2h_bytes_per_step": int(yh.numel() * 4),
                     "ms_per_step": e2e_ms},
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
-            "plan": st,
+            "plan": a.plan.stats,
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(a, x.cpu().numpy(), b_alg)

@@ -19,6 +19,7 @@ NOALLOC_MAX_ROWS = 1048544
 F32, BF16 = 0, 1
 OP_AX, OP_ADX, OP_DADX, OP_VALUES_ADD, OP_VALUES_RATIO, OP_DAD_ADD = range(6)
 INPUT_DEVICE, INPUT_HOST = 0, 1
+VARIANT_AUTO, VARIANT_REGISTER, VARIANT_STAGED = 0, 1, 2
 BUILD_EXHAUSTIVE = 1
 S_DELTA_ROW, S_DELTA_COL, S_DELTA_VAL, S_BRANCHES, S_SRC, S_DST, S_PARENT, S_CSR_PTR, S_CSR_COL, \
     S_CSR_VAL = range(10)
@@ -40,7 +41,7 @@ SIGNATURES = [
     ("cbm_plan_create", C.c_int, [vp, vp, vp, i64, i64, i64, vp, i64, vp, vp, i64, vp, i32, vp,
                                   C.POINTER(vp)]),
     ("cbm_plan_set_multipliers", C.c_int, [vp, vp, vp]),
-    ("cbm_plan_tune", C.c_int, [vp, i32, i32, vp]),
+    ("cbm_plan_tune", C.c_int, [vp, i32, i32, i32, i64, i32, vp]),
     ("cbm_plan_workspace_bytes", i64, [vp, i32, i64, i32, i32, i32]),
     ("cbm_matmul", C.c_int, [vp, i32, vp, i32, i64, vp, i32, i64, i64, vp, i64, vp]),
     ("cbm_matmul_adjoint", C.c_int, [vp, i32, vp, i32, i64, vp, i32, i64, i64, vp, i64, vp]),

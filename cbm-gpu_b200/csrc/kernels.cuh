@@ -21,10 +21,16 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <climits>
 
 namespace cbm {
 
 constexpr int kThreads = 256;
+
+// Forward entry word: column in bits 0-29, bit 30 set for the columns gathered
+// most often (L2 keeps their X rows), bit 31 the sign.
+constexpr uint32_t kColMask = 0x3fffffffu;
+constexpr uint32_t kHotBit = 0x40000000u;
 
 enum ScaleMode : int {
   SCALE_SIGN = 0,       // s
@@ -52,10 +58,13 @@ struct FwdArgs {
   const uint32_t* ent;       // column | sign << 31
   const float* val;          // values (SCALE_VALUES) or null
   const int32_t* par;        // parent node id, -1 for children of the virtual root
+  const int32_t* par_item;   // queue position of the parent's item, -1
   const int32_t* self_slot;  // internal-node slot of the item's node, -1 if leaf
   const int32_t* par_slot;   // internal-node slot of the parent, -1
   const int32_t* chunk0;     // first chunk of a split row, -1
-  // chunks of long rows
+  // chunks of long rows (entries in cent / cval)
+  const uint32_t* cent;
+  const float* cval;
   int32_t n_chunks;
   const int32_t* chunk_item;
   const int64_t* chunk_beg;
@@ -78,6 +87,7 @@ struct FwdArgs {
   int32_t prop_mode;
   int32_t team;        // lanes per row: 1, 2, 4, 8, 16 or 32
   int32_t rows_per_claim;
+  int32_t hints;       // L2 cache policies on (staged kernel)
   long long timeout_ns;
 };
 
@@ -182,6 +192,23 @@ __device__ __forceinline__ void store_vec<__nv_bfloat16, 1>(__nv_bfloat16* p, co
   *p = __float2bfloat16_rn(v[0]);
 }
 
+// evict-first (streaming) stores of V floats as T
+template <typename T, int V>
+__device__ __forceinline__ void store_vec_cs(T* p, const float (&v)[V]) {
+  if constexpr (sizeof(T) == 4 && V % 4 == 0) {
+#pragma unroll
+    for (int i = 0; i < V / 4; ++i)
+      __stcs(reinterpret_cast<float4*>(p) + i, make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]));
+  } else if constexpr (sizeof(T) == 2 && V == 8) {
+    __nv_bfloat162 h[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) h[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+    __stcs(reinterpret_cast<uint4*>(p), *reinterpret_cast<const uint4*>(h));
+  } else {
+    store_vec<T, V>(p, v);
+  }
+}
+
 // fp32 scratch rows (partials, parent state): L2-coherent loads after an acquire
 template <int V>
 __device__ __forceinline__ void load_f32_cg(const float* p, float (&o)[V]) {
@@ -238,7 +265,7 @@ __device__ __forceinline__ void gather_range(float (&acc)[VPL][V], const XT* __r
     float sc = 0.f;
     if (idx < end) {
       e = __ldg(ent + idx);
-      const uint32_t c = e & 0x7fffffffu;
+      const uint32_t c = e & kColMask;
       const float sgn = (e >> 31) ? -1.f : 1.f;
       if (scale_mode == SCALE_SIGN) {
         sc = sgn;
@@ -258,7 +285,7 @@ __device__ __forceinline__ void gather_range(float (&acc)[VPL][V], const XT* __r
       for (int u = 0; u < U; ++u) {
         const uint32_t eu = __shfl_sync(tmask, e, j + u < cnt ? j + u : 0, TL);
         s[u] = __shfl_sync(tmask, sc, j + u < cnt ? j + u : 0, TL);
-        const XT* row = x + (int64_t)(eu & 0x7fffffffu) * ldx;
+        const XT* row = x + (int64_t)(eu & kColMask) * ldx;
 #pragma unroll
         for (int v = 0; v < VPL; ++v) {
           const int vi = tl + v * TL;
@@ -293,7 +320,7 @@ __device__ __forceinline__ void fwd_chunk(const FwdArgs& a, int k, unsigned epoc
   const int item = a.chunk_item[k];
   const int node = a.node[item] & 0x7fffffff;
   const float dv = (a.scale_mode == SCALE_DCOL_DROW) ? __ldg(a.mult + node) : 1.f;
-  gather_range<XT, VPL, V>(acc, static_cast<const XT*>(a.x), a.ldx, a.nvec, a.ent, a.val, a.chunk_beg[k],
+  gather_range<XT, VPL, V>(acc, static_cast<const XT*>(a.x), a.ldx, a.nvec, a.cent, a.cval, a.chunk_beg[k],
                            a.chunk_end[k], a.scale_mode, a.mult, dv, tl, TL, tmask);
   float* prow = a.partial + (int64_t)k * a.ldp;
 #pragma unroll
@@ -432,6 +459,350 @@ __global__ void __launch_bounds__(kThreads) fwd_kernel(const FwdArgs a) {
       fwd_row<XT, YT, VPL, V>(a, (int)item, epoch, tl, TL, tmask);
     }
     __syncwarp();
+  }
+  finish_block(a.qs, epoch);
+}
+
+// ============================================================================
+// Staged variant of the forward kernel (16-byte vector path, teams of >= 8
+// lanes).  The work a team claims is a run of consecutive items, and the
+// stream layout stores their entries contiguously, so the team walks one flat
+// entry range.  X rows are fetched with cp.async into a per-thread ring of S
+// slots in shared memory, S entries ahead of the consumer, independent of row
+// boundaries: S gathers stay in flight without holding registers.  Each lane
+// copies and later reads only its own 16-byte pieces, so the only waits are
+// the lane's own cp.async groups.  Column indices come in batches of TL (one
+// coalesced load per batch), three batches in flight; the items' metadata for
+// a claim is held one item per lane.  Rows are finished (chunk partials,
+// parent, store, ready flag) when the consumer crosses their end.
+// ============================================================================
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async16_hint(void* smem, const void* gmem, uint64_t policy) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;" ::"r"(s), "l"(gmem), "l"(policy)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <typename XT, int V>
+__device__ __forceinline__ void unpack16(const uint4& r, float (&o)[V]) {
+  if constexpr (sizeof(XT) == 4) {
+    o[0] = __uint_as_float(r.x);
+    o[1] = __uint_as_float(r.y);
+    o[2] = __uint_as_float(r.z);
+    o[3] = __uint_as_float(r.w);
+  } else {
+    const uint32_t w[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      o[2 * i] = __uint_as_float(w[i] << 16);
+      o[2 * i + 1] = __uint_as_float(w[i] & 0xffff0000u);
+    }
+  }
+}
+
+// Scale of one entry before the row factor: s, s * m[col] (both for
+// SCALE_DCOL and SCALE_DCOL_DROW, whose consumer then multiplies by m[row]) or
+// the stored value.
+__device__ __forceinline__ float entry_scale(uint32_t e, int64_t idx, bool valid, int scale_mode, const float* mult,
+                                             const float* val) {
+  if (!valid) return 0.f;
+  const float sgn = (e >> 31) ? -1.f : 1.f;
+  if (scale_mode == SCALE_SIGN) return sgn;
+  if (scale_mode == SCALE_VALUES) return __ldg(val + idx);
+  return sgn * __ldg(mult + (e & kColMask));
+}
+
+// One team's pipelined pass over the `len` entries ent[k0, k0 + len).  With
+// lockstep every lane of the warp calls it (a team with nothing to do passes
+// len = 0).
+// Positions are 32-bit and relative to k0; batches of TL entries start at
+// multiples of TL.  next_end() gives the relative position where the
+// current item ends (INT_MAX when none is left); on_end(acc) finishes it,
+// resets acc and advances, updating row_dv (the row factor of SCALE_DCOL_DROW).
+template <typename XT, int TL, int VPL, int V, int S, int BLOCK, typename NextEnd, typename OnEnd>
+__device__ __forceinline__ void stream_pass(const XT* __restrict__ x, int64_t ldx, int nvec,
+                                            const uint32_t* __restrict__ ent, const float* __restrict__ val,
+                                            int64_t k0, int len, int scale_mode, const float* __restrict__ mult,
+                                            uint4* __restrict__ ring, int tl, unsigned tmask, NextEnd next_end,
+                                            OnEnd on_end, const float& row_dv, bool hints, bool lockstep) {
+  static_assert(S <= TL && TL % S == 0, "ring depth must divide the team size");
+  uint64_t pol_keep, pol_stream;
+  if (hints) {
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol_keep));
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol_stream));
+  } else {
+    asm volatile("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(pol_keep));
+    pol_stream = pol_keep;
+  }
+  const uint32_t* ent0 = ent + k0;
+  const float* val0 = val ? val + k0 : nullptr;
+  const XT* xl = x + (int64_t)tl * V;  // this lane's first element of any row
+  uint4* my = ring + threadIdx.x;      // this thread's ring: slot s, piece v at my[(s * VPL + v) * BLOCK]
+  bool piece_ok[VPL];
+#pragma unroll
+  for (int v = 0; v < VPL; ++v) piece_ok[v] = tl + v * TL < nvec;
+
+  // three batches of TL entries: A (holds the consumer position), B, C
+  int bA = 0;
+  uint32_t eA = 0, eB = 0, eC = 0;
+  float sA = 0.f, sB = 0.f;
+  {
+    const int ia = tl, ib = TL + tl, ic = 2 * TL + tl;
+    if (ia < len) eA = __ldcs(ent0 + ia);
+    if (ib < len) eB = __ldcs(ent0 + ib);
+    if (ic < len) eC = __ldcs(ent0 + ic);
+    sA = entry_scale(eA, ia, ia < len, scale_mode, mult, val0);
+    sB = entry_scale(eB, ib, ib < len, scale_mode, mult, val0);
+  }
+  auto produce = [&](int p, uint4* sp) {
+    if (p < len) {
+      const bool inA = p < bA + TL;
+      const uint32_t e = __shfl_sync(tmask, inA ? eA : eB, p & (TL - 1), TL);
+      const XT* row = xl + (int64_t)(e & kColMask) * ldx;
+      const uint64_t pol = (e & kHotBit) ? pol_keep : pol_stream;
+#pragma unroll
+      for (int v = 0; v < VPL; ++v)
+        if (piece_ok[v]) cp_async16_hint(sp + v * BLOCK, row + v * TL * V, pol);
+    }
+    cp_async_commit();
+  };
+#pragma unroll
+  for (int j = 0; j < S; ++j) produce(j, my + j * (VPL * BLOCK));
+
+  float acc[VPL][V];
+#pragma unroll
+  for (int v = 0; v < VPL; ++v)
+#pragma unroll
+    for (int q = 0; q < V; ++q) acc[v][q] = 0.f;
+  int end_at = next_end();
+  int slot = 0;
+  // With lockstep, all teams of the warp step together (to the warp's longest
+  // stream) so that one instruction serves every team, finished teams idling.
+  // Only when no team waits on a row another team of the warp produces in the
+  // same pass (the caller checks): a wait would then block the producer at
+  // the per-step warp barrier.
+  const int wlen = lockstep ? __reduce_max_sync(0xffffffffu, len) : len;
+  for (int k = 0; k < wlen; ++k) {
+    const bool active = k < len;
+    if (active) {
+      while (k == end_at) {
+        on_end(acc);
+        end_at = next_end();
+      }
+    }
+    if (k == bA + TL) {
+      // rotate: A <- B (scales ready), B <- C (scales now), load a new C
+      bA += TL;
+      eA = eB;
+      sA = sB;
+      eB = eC;
+      const int ib = bA + TL + tl, ic = bA + 2 * TL + tl;
+      sB = entry_scale(eB, ib, ib < len, scale_mode, mult, val0);
+      eC = ic < len ? __ldcs(ent0 + ic) : 0u;
+    }
+    cp_async_wait<S - 1>();
+    float sc = __shfl_sync(tmask, sA, k & (TL - 1), TL);
+    if (scale_mode == SCALE_DCOL_DROW) sc = __fmul_rn(sc, row_dv);
+    if (!active) sc = 0.f;
+    uint4* sp = my + slot * (VPL * BLOCK);
+#pragma unroll
+    for (int v = 0; v < VPL; ++v) {
+      if (piece_ok[v] && active) {
+        float t[V];
+        unpack16<XT, V>(sp[v * BLOCK], t);
+#pragma unroll
+        for (int q = 0; q < V; ++q) acc[v][q] = fmaf(sc, t[q], acc[v][q]);
+      }
+    }
+    produce(k + S, sp);
+    slot = (slot + 1 == S) ? 0 : slot + 1;
+    if (lockstep) __syncwarp();
+  }
+  cp_async_wait<0>();
+  while (end_at <= len) {
+    on_end(acc);
+    end_at = next_end();
+  }
+  if (lockstep) __syncwarp();
+}
+
+template <typename XT, typename YT, int TL, int VPL, int V, int S, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) fwd_stream_kernel(const FwdArgs a) {
+  extern __shared__ uint4 ring[];
+  const int lane = threadIdx.x & 31;
+  const int team = lane / TL;
+  const int tl = lane & (TL - 1);
+  constexpr int teams = 32 / TL;
+  const unsigned tmask = (TL == 32) ? 0xffffffffu : (((1u << TL) - 1u) << (team * TL));
+  const unsigned epoch = *(volatile unsigned*)&a.qs->epoch + 1u;
+  const XT* x = static_cast<const XT*>(a.x);
+  const bool hints = a.hints != 0;
+  float ch_dv = 1.f;
+
+  // ---- chunks of long rows: one chunk per team per claim ----
+  if (a.n_chunks > 0) {
+    for (;;) {
+      unsigned base = 0;
+      if (lane == 0) base = atomicAdd(&a.qs->next_chunk, (unsigned)teams);
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (base >= (unsigned)a.n_chunks) break;
+      const unsigned k = base + team;
+      const bool have = k < (unsigned)a.n_chunks;
+      int64_t cb = 0;
+      int clen = 0;
+      if (have) {
+        const int item = a.chunk_item[k];
+        const int node = a.node[item] & 0x7fffffff;
+        ch_dv = (a.scale_mode == SCALE_DCOL_DROW) ? __ldg(a.mult + node) : 1.f;
+        cb = a.chunk_beg[k];
+        clen = (int)(a.chunk_end[k] - cb);
+      }
+      bool done = !have;
+      auto next_end = [&]() -> int { return done ? INT_MAX : clen; };
+      auto on_end = [&](float (&acc)[VPL][V]) {
+        float* prow = a.partial + (int64_t)k * a.ldp;
+#pragma unroll
+        for (int v = 0; v < VPL; ++v) {
+          const int vi = tl + v * TL;
+          if (vi < a.nvec) store_f32<V>(prow + vi * V, acc[v]);
+        }
+        __threadfence();
+        __syncwarp(tmask);
+        if (tl == 0) st_release(a.chunk_flag + k, epoch);
+        done = true;
+      };
+      // chunks depend on nothing: always in lockstep
+      stream_pass<XT, TL, VPL, V, S, BLOCK>(x, a.ldx, a.nvec, a.cent, a.cval, cb, clen, a.scale_mode, a.mult,
+                                            ring, tl, tmask, next_end, on_end, ch_dv, hints, true);
+    }
+  }
+
+  // ---- rows: a team takes R consecutive items per claim ----
+  const int R = a.rows_per_claim < TL ? a.rows_per_claim : TL;
+  const unsigned per_claim = (unsigned)(teams * R);
+  const bool need_dv = (a.scale_mode == SCALE_DCOL_DROW) || (a.prop_mode == PROP_RATIO);
+  for (;;) {
+    unsigned base = 0;
+    if (lane == 0) base = atomicAdd(&a.qs->next_row, per_claim);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= (unsigned)a.n_items) break;
+    const int64_t i0 = (int64_t)base + (int64_t)team * R;
+    {
+      const int64_t i1 = (i0 + R < a.n_items) ? i0 + R : a.n_items;
+      const int nit = i0 < a.n_items ? (int)(i1 - i0) : 0;
+      const int64_t k0 = nit > 0 ? a.ptr[i0] : 0;
+      // item metadata, one item per lane; ends relative to k0
+      int m_node = 0, m_par = -1, m_chunk = -1, m_pslot = -1, m_sslot = -1, m_end = 0;
+      float m_dv = 1.f;
+      bool dep_in_claim = false;
+      if (tl < nit) {
+        const int64_t it = i0 + tl;
+        m_node = a.node[it];
+        m_par = a.par[it];
+        dep_in_claim = m_par >= 0 && a.par_item[it] >= (int)base;
+        m_chunk = a.chunk0[it];
+        m_pslot = a.par_slot[it];
+        m_sslot = a.self_slot[it];
+        m_end = (int)(a.ptr[it + 1] - k0);
+        if (need_dv) m_dv = __ldg(a.mult + (m_node & 0x7fffffff));
+      }
+      const int len = nit > 0 ? __shfl_sync(tmask, m_end, nit - 1, TL) : 0;
+      int cur = 0;  // item (relative) the consumer is in
+      float row_dv = __shfl_sync(tmask, m_dv, 0, TL);
+      auto next_end = [&]() -> int { return cur < nit ? __shfl_sync(tmask, m_end, cur, TL) : INT_MAX; };
+      auto on_end = [&](float (&acc)[VPL][V]) {
+        const int nodew = __shfl_sync(tmask, m_node, cur, TL);
+        const int node = nodew & 0x7fffffff;
+        const int c0 = __shfl_sync(tmask, m_chunk, cur, TL);
+        const int p = __shfl_sync(tmask, m_par, cur, TL);
+        const int ps = __shfl_sync(tmask, m_pslot, cur, TL);
+        const int ss = __shfl_sync(tmask, m_sslot, cur, TL);
+        const float dv = row_dv;
+        if (c0 >= 0) {
+          const int item = (int)(i0 + cur);
+          for (int k = c0; k < a.n_chunks && a.chunk_item[k] == item; ++k) {
+            if (!wait_flag(a.chunk_flag + k, epoch, a.qs, a.timeout_ns, (long long)k)) continue;
+            const float* prow = a.partial + (int64_t)k * a.ldp;
+#pragma unroll
+            for (int v = 0; v < VPL; ++v) {
+              const int vi = tl + v * TL;
+              if (vi < a.nvec) {
+                float t[V];
+                load_f32_cg<V>(prow + vi * V, t);
+#pragma unroll
+                for (int q = 0; q < V; ++q) acc[v][q] = __fadd_rn(acc[v][q], t[q]);
+              }
+            }
+          }
+        }
+        if (p >= 0 && wait_flag(a.node_flag + p, epoch, a.qs, a.timeout_ns, (long long)node)) {
+          const float dp = (a.prop_mode == PROP_RATIO) ? __ldg(a.mult + p) : 1.f;
+#pragma unroll
+          for (int v = 0; v < VPL; ++v) {
+            const int vi = tl + v * TL;
+            if (vi < a.nvec) {
+              float yp[V];
+              if constexpr (sizeof(YT) == 4) {
+                load_y_cg<YT, V>(static_cast<const YT*>(a.y) + (int64_t)p * a.ldy + (int64_t)vi * V, yp);
+              } else {
+                load_f32_cg<V>(a.pstate + (int64_t)ps * a.ldp + vi * V, yp);
+              }
+              if (a.prop_mode == PROP_RATIO) {
+#pragma unroll
+                for (int q = 0; q < V; ++q) acc[v][q] = __fadd_rn(acc[v][q], __fdiv_rn(__fmul_rn(yp[q], dv), dp));
+              } else {
+#pragma unroll
+                for (int q = 0; q < V; ++q) acc[v][q] = __fadd_rn(acc[v][q], yp[q]);
+              }
+            }
+          }
+        }
+        YT* yrow = static_cast<YT*>(a.y) + (int64_t)node * a.ldy;
+        // leaves are not read again by this kernel: stream them past L2
+        const bool stream_y = hints && nodew >= 0;
+#pragma unroll
+        for (int v = 0; v < VPL; ++v) {
+          const int vi = tl + v * TL;
+          if (vi < a.nvec) {
+            if (stream_y)
+              store_vec_cs<YT, V>(yrow + (int64_t)vi * V, acc[v]);
+            else
+              store_vec<YT, V>(yrow + (int64_t)vi * V, acc[v]);
+          }
+        }
+        if (nodew < 0) {
+          if constexpr (sizeof(YT) != 4) {
+            float* srow = a.pstate + (int64_t)ss * a.ldp;
+#pragma unroll
+            for (int v = 0; v < VPL; ++v) {
+              const int vi = tl + v * TL;
+              if (vi < a.nvec) store_f32<V>(srow + vi * V, acc[v]);
+            }
+          }
+          __threadfence();
+          __syncwarp(tmask);
+          if (tl == 0) st_release(a.node_flag + node, epoch);
+        }
+#pragma unroll
+        for (int v = 0; v < VPL; ++v)
+#pragma unroll
+          for (int q = 0; q < V; ++q) acc[v][q] = 0.f;
+        ++cur;
+        row_dv = __shfl_sync(tmask, m_dv, cur < nit ? cur : 0, TL);
+      };
+      // a parent row inside this warp's claim: let the teams run independently
+      const bool lockstep = !__any_sync(0xffffffffu, dep_in_claim);
+      stream_pass<XT, TL, VPL, V, S, BLOCK>(x, a.ldx, a.nvec, a.ent, a.val, k0, len, a.scale_mode, a.mult, ring,
+                                            tl, tmask, next_end, on_end, row_dv, hints, lockstep);
+    }
   }
   finish_block(a.qs, epoch);
 }

@@ -92,6 +92,78 @@ int launch_fwd_t(cbm_plan* P, const FwdArgs& a, cudaStream_t st) {
   return cuda_status(cudaGetLastError());
 }
 
+// Staged kernel: ring of S slots of VPL 16-byte pieces per thread, blocks of
+// 128 threads.
+constexpr int kStagedBlock = 128;
+
+template <typename XT, typename YT, int TL, int VPL, int V, int S>
+int launch_stream_t(cbm_plan* P, const FwdArgs& a, cudaStream_t st) {
+  static int grid_cache = 0, grid_dev = -1;
+  constexpr int smem = S * VPL * kStagedBlock * 16;
+  auto kern = fwd_stream_kernel<XT, YT, TL, VPL, V, S, kStagedBlock>;
+  if (grid_dev != P->device) {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+      return CBM_ERR_CUDA;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kStagedBlock, smem) != cudaSuccess ||
+        per_sm < 1)
+      per_sm = 1;
+    grid_cache = per_sm * sm_count(P->device);
+    grid_dev = P->device;
+  }
+  kern<<<grid_cache, kStagedBlock, smem, st>>>(a);
+  P->launches++;
+  P->last_grid = grid_cache;
+  return cuda_status(cudaGetLastError());
+}
+
+// Team shape of the staged kernel for nvec 16-byte pieces per row.  A lane
+// holds at most 32 accumulators (8 pieces of fp32, 4 of bf16).  Default: the
+// widest team up to a full warp (one row stream per warp when the row has >= 32
+// pieces; narrower rows share a warp between streams that step together);
+// `forced` (8, 16 or 32) overrides it where the pieces fit.
+bool staged_shape(int64_t nvec, int v, int forced, int* team, int* vpl) {
+  const int max_vpl = 32 / v;
+  if (nvec < 8 || nvec > 32 * max_vpl) return false;
+  int t = 8;
+  while (t < 32 && t < nvec) t <<= 1;
+  if (forced != 0) {
+    if (forced * max_vpl < nvec) return false;
+    t = forced;
+  }
+  int p = 1;
+  while (t * p < nvec) p <<= 1;
+  *team = t;
+  *vpl = p;
+  return true;
+}
+
+template <typename XT, typename YT, int TL>
+int launch_staged_team(cbm_plan* P, const FwdArgs& a, int vpl, cudaStream_t st) {
+  constexpr int V = 16 / (int)sizeof(XT);
+  switch (vpl) {
+    case 1: return launch_stream_t<XT, YT, TL, 1, V, 8>(P, a, st);
+    case 2: return launch_stream_t<XT, YT, TL, 2, V, 8>(P, a, st);
+    case 4: return launch_stream_t<XT, YT, TL, 4, V, 8>(P, a, st);
+    default:
+      if constexpr (V == 4) return launch_stream_t<XT, YT, TL, 8, V, 4>(P, a, st);
+      return CBM_ERR_INTERNAL;
+  }
+}
+
+template <typename XT, typename YT>
+int launch_staged_any(cbm_plan* P, const FwdArgs& a, int team, int vpl, cudaStream_t st) {
+  if (team == 8) return launch_staged_team<XT, YT, 8>(P, a, vpl, st);
+  if (team == 16) return launch_staged_team<XT, YT, 16>(P, a, vpl, st);
+  return launch_staged_team<XT, YT, 32>(P, a, vpl, st);
+}
+
+int launch_staged(cbm_plan* P, const FwdArgs& a, int32_t xdt, int32_t ydt, int team, int vpl, cudaStream_t st) {
+  if (xdt == CBM_F32) return launch_staged_any<float, float>(P, a, team, vpl, st);
+  if (ydt == CBM_F32) return launch_staged_any<__nv_bfloat16, float>(P, a, team, vpl, st);
+  return launch_staged_any<__nv_bfloat16, __nv_bfloat16>(P, a, team, vpl, st);
+}
+
 template <typename XT, typename YT, int V>
 int launch_fwd_v(cbm_plan* P, const FwdArgs& a, int vpl, cudaStream_t st) {
   switch (vpl) {
@@ -328,6 +400,11 @@ int cbm_plan_debug_set_parent(cbm_plan* P, int64_t item, int32_t parent_node, vo
   const int32_t zero = 0;
   if (cudaMemcpyAsync(P->d_par_slot + item, &zero, sizeof(int32_t), cudaMemcpyHostToDevice, st) != cudaSuccess)
     return CBM_ERR_CUDA;
+  int32_t par_item = -1;
+  for (int64_t i = 0; parent_node >= 0 && i < P->n_items; ++i)
+    if (P->h_order[i] == parent_node) par_item = (int32_t)i;
+  if (cudaMemcpyAsync(P->d_par_item + item, &par_item, sizeof(int32_t), cudaMemcpyHostToDevice, st) != cudaSuccess)
+    return CBM_ERR_CUDA;
   return cuda_status(cudaStreamSynchronize(st));
 }
 
@@ -374,7 +451,10 @@ int cbm_matmul(cbm_plan* P, int32_t op, const void* x, int32_t xdt, int64_t ldx,
     a.ptr = P->d_ptr;
     a.ent = P->d_ent;
     a.val = P->d_val;
+    a.cent = P->d_cent;
+    a.cval = P->d_cval;
     a.par = P->d_par;
+    a.par_item = P->d_par_item;
     a.self_slot = P->d_self_slot;
     a.par_slot = P->d_par_slot;
     a.chunk0 = P->d_chunk0;
@@ -398,8 +478,18 @@ int cbm_matmul(cbm_plan* P, int32_t op, const void* x, int32_t xdt, int64_t ldx,
     a.prop_mode = prop;
     a.team = team;
     a.rows_per_claim = P->rows_per_claim;
+    a.hints = P->hot_rows > 0 ? 1 : 0;
     a.timeout_ns = P->timeout_ns;
-    const int rc = launch_fwd(P, a, xdt, ydt, sh.vec, vpl, st);
+    int s_team = 0, s_vpl = 0;
+    const bool staged = sh.vec && P->variant != CBM_VARIANT_REGISTER &&
+                        staged_shape(nvec, sh.v, P->staged_team, &s_team, &s_vpl);
+    int rc;
+    if (staged) {
+      a.team = s_team;
+      rc = launch_staged(P, a, xdt, ydt, s_team, s_vpl, st);
+    } else {
+      rc = launch_fwd(P, a, xdt, ydt, sh.vec, vpl, st);
+    }
     if (rc) return rc;
   }
   return CBM_OK;

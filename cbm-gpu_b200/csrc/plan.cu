@@ -108,29 +108,74 @@ int validate_structure(const int32_t* rp, const int32_t* ci, int64_t n_rows, int
   return CBM_OK;
 }
 
-// Builds the chunk table for the current chunk size and uploads it.
-int build_chunks(cbm_plan* P, cudaStream_t st) {
+// Builds the device stream layout for the current chunk size and uploads it:
+// rows no longer than chunk_nnz keep their entries in s_ent, contiguous in
+// item order (so a run of consecutive items is one contiguous entry range);
+// longer rows have no entries there and are summed from c_ent in chunks of
+// chunk_nnz entries.
+int build_layout(cbm_plan* P, cudaStream_t st) {
   free_all(P->chunk_bufs);
-  std::vector<int32_t> chunk0(P->n_items, -1), citem;
-  std::vector<int64_t> cbeg, cend;
-  int64_t long_rows = 0;
+  const int64_t n = P->n_items;
   const int64_t T = P->chunk_nnz;
-  for (int64_t i = 0; i < P->n_items; ++i) {
-    const int64_t b = P->h_ptr[i], e = P->h_ptr[i + 1];
-    if (e - b > T) {
+  const bool vals = !P->h_val.empty();
+  std::vector<int64_t> sptr(n + 1, 0);
+  std::vector<int32_t> chunk0(n, -1), citem;
+  std::vector<int64_t> cbeg, cend;
+  int64_t long_rows = 0, long_nnz = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    const int64_t len = P->h_ptr[i + 1] - P->h_ptr[i];
+    const bool is_long = len > T;
+    sptr[i + 1] = sptr[i] + (is_long ? 0 : len);
+    if (is_long) {
       ++long_rows;
       chunk0[i] = (int32_t)citem.size();
-      for (int64_t s = b; s < e; s += T) {
+      for (int64_t s = 0; s < len; s += T) {
         citem.push_back((int32_t)i);
-        cbeg.push_back(s);
-        cend.push_back(std::min(e, s + T));
+        cbeg.push_back(long_nnz + s);
+        cend.push_back(long_nnz + std::min(len, s + T));
       }
+      long_nnz += len;
     }
   }
   if (citem.size() > (size_t)INT32_MAX) return CBM_ERR_INVALID;
+  // the hot_rows columns gathered most often get the hot bit (their X rows are
+  // kept in L2 by the staged kernel)
+  std::vector<uint32_t> hot(P->n_cols, 0u);
+  if (P->hot_rows > 0 && P->n_cols > 0) {
+    std::vector<int64_t> freq(P->n_cols, 0);
+    for (uint32_t e : P->h_ent) freq[e & 0x3fffffffu]++;
+    std::vector<int32_t> by(P->n_cols);
+    for (int64_t c = 0; c < P->n_cols; ++c) by[c] = (int32_t)c;
+    const int64_t k = std::min<int64_t>(P->hot_rows, P->n_cols);
+    std::nth_element(by.begin(), by.begin() + (k - 1), by.end(),
+                     [&](int32_t a, int32_t b) { return freq[a] > freq[b] || (freq[a] == freq[b] && a < b); });
+    for (int64_t i = 0; i < k; ++i)
+      if (freq[by[i]] > 1) hot[by[i]] = 0x40000000u;
+  }
+  std::vector<uint32_t> sent(sptr[n]), cent(long_nnz);
+  std::vector<float> sval(vals ? sptr[n] : 0), cval(vals ? long_nnz : 0);
+  for (int64_t i = 0, lo = 0; i < n; ++i) {
+    const int64_t b = P->h_ptr[i], len = P->h_ptr[i + 1] - b;
+    uint32_t* out = chunk0[i] >= 0 ? cent.data() + lo : sent.data() + sptr[i];
+    for (int64_t q = 0; q < len; ++q) {
+      const uint32_t e = P->h_ent[b + q];
+      out[q] = e | hot[e & 0x3fffffffu];
+    }
+    if (chunk0[i] >= 0) {
+      if (vals) std::memcpy(cval.data() + lo, P->h_val.data() + b, len * sizeof(float));
+      lo += len;
+    } else {
+      if (vals) std::memcpy(sval.data() + sptr[i], P->h_val.data() + b, len * sizeof(float));
+    }
+  }
   P->n_chunks = (int64_t)citem.size();
   P->long_rows = long_rows;
   int rc;
+  if ((rc = dev_upload(&P->d_ptr, sptr, st, P->chunk_bufs))) return rc;
+  if ((rc = dev_upload(&P->d_ent, sent, st, P->chunk_bufs))) return rc;
+  if ((rc = dev_upload(&P->d_val, sval, st, P->chunk_bufs))) return rc;
+  if ((rc = dev_upload(&P->d_cent, cent, st, P->chunk_bufs))) return rc;
+  if ((rc = dev_upload(&P->d_cval, cval, st, P->chunk_bufs))) return rc;
   if ((rc = dev_upload(&P->d_chunk0, chunk0, st, P->chunk_bufs))) return rc;
   if ((rc = dev_upload(&P->d_chunk_item, citem, st, P->chunk_bufs))) return rc;
   if ((rc = dev_upload(&P->d_chunk_beg, cbeg, st, P->chunk_bufs))) return rc;
@@ -190,7 +235,7 @@ int cbm_plan_create(const int32_t* row_ptr, const int32_t* col_idx, const float*
   if (!out) return CBM_ERR_INVALID;
   *out = nullptr;
   if (n_rows < 0 || n_cols < 0 || nnz < 0 || n_edges < 0 || n_branch_offsets < 0) return CBM_ERR_INVALID;
-  if (n_rows >= INT32_MAX || n_cols >= INT32_MAX) return CBM_ERR_INVALID;
+  if (n_rows >= (int64_t)1 << 30 || n_cols >= (int64_t)1 << 30) return CBM_ERR_INVALID;  // 30-bit column field
   if (input_kind != CBM_INPUT_DEVICE && input_kind != CBM_INPUT_HOST) return CBM_ERR_INVALID;
   const bool dev = input_kind == CBM_INPUT_DEVICE;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -252,7 +297,9 @@ int cbm_plan_create(const int32_t* row_ptr, const int32_t* col_idx, const float*
   P->n_internal = n_internal;
 
   P->n_items = n_rows;
-  std::vector<int32_t> item_node(n_rows), item_par(n_rows), item_self_slot(n_rows), item_par_slot(n_rows);
+  std::vector<int32_t> item_node(n_rows), item_par(n_rows), item_self_slot(n_rows), item_par_slot(n_rows),
+      item_par_item(n_rows), item_of(n_rows);
+  for (int64_t i = 0; i < n_rows; ++i) item_of[order[i]] = (int32_t)i;
   P->h_ptr.assign(n_rows + 1, 0);
   for (int64_t i = 0; i < n_rows; ++i) {
     const int32_t v = order[i];
@@ -260,6 +307,7 @@ int cbm_plan_create(const int32_t* row_ptr, const int32_t* col_idx, const float*
     item_par[i] = parent[v];
     item_self_slot[i] = slot[v];
     item_par_slot[i] = parent[v] >= 0 ? slot[parent[v]] : -1;
+    item_par_item[i] = parent[v] >= 0 ? item_of[parent[v]] : -1;
     P->h_ptr[i + 1] = P->h_ptr[i] + (rp[v + 1] - rp[v]);
   }
   bool unit = true;
@@ -287,14 +335,13 @@ int cbm_plan_create(const int32_t* row_ptr, const int32_t* col_idx, const float*
   P->h_parent = parent;
   P->h_slot = slot;
   P->h_depth = depth;
-  P->h_ent = ent;
+  P->h_ent.swap(ent);
+  P->h_val.swap(lval);
 
   // ---- upload ----
   if ((rc = dev_upload(&P->d_node, item_node, st, P->bufs))) return fail(rc);
-  if ((rc = dev_upload(&P->d_ptr, P->h_ptr, st, P->bufs))) return fail(rc);
-  if ((rc = dev_upload(&P->d_ent, ent, st, P->bufs))) return fail(rc);
-  if ((rc = dev_upload(&P->d_val, lval, st, P->bufs))) return fail(rc);
   if ((rc = dev_upload(&P->d_par, item_par, st, P->bufs))) return fail(rc);
+  if ((rc = dev_upload(&P->d_par_item, item_par_item, st, P->bufs))) return fail(rc);
   if ((rc = dev_upload(&P->d_self_slot, item_self_slot, st, P->bufs))) return fail(rc);
   if ((rc = dev_upload(&P->d_par_slot, item_par_slot, st, P->bufs))) return fail(rc);
   if (!mult.empty()) {
@@ -312,7 +359,7 @@ int cbm_plan_create(const int32_t* row_ptr, const int32_t* col_idx, const float*
     if (cudaMemsetAsync(f, 0, sizeof(QueueState), st) != cudaSuccess) return fail(CBM_ERR_CUDA);
     P->d_qs = static_cast<QueueState*>(f);
   }
-  if ((rc = build_chunks(P, st))) return fail(rc);
+  if ((rc = build_layout(P, st))) return fail(rc);
   *out = P;
   return CBM_OK;
 }
@@ -332,14 +379,20 @@ int cbm_plan_set_multipliers(cbm_plan* P, const float* d_mult, void* stream) {
   return CBM_OK;
 }
 
-int cbm_plan_tune(cbm_plan* P, int32_t chunk_nnz, int32_t rows_per_claim, void* stream) {
-  if (!P || chunk_nnz < 32 || rows_per_claim < 1 || rows_per_claim > 1024) return CBM_ERR_INVALID;
+int cbm_plan_tune(cbm_plan* P, int32_t chunk_nnz, int32_t rows_per_claim, int32_t variant, int64_t hot_rows,
+                  int32_t team, void* stream) {
+  if (!P || chunk_nnz < 32 || rows_per_claim < 1 || rows_per_claim > 1024 || hot_rows < 0) return CBM_ERR_INVALID;
+  if (team != 0 && team != 8 && team != 16 && team != 32) return CBM_ERR_INVALID;
+  P->staged_team = team;
+  if (variant < CBM_VARIANT_AUTO || variant > CBM_VARIANT_STAGED) return CBM_ERR_INVALID;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (cudaStreamSynchronize(st) != cudaSuccess) return CBM_ERR_CUDA;
   P->rows_per_claim = rows_per_claim;
-  if (chunk_nnz != P->chunk_nnz) {
+  P->variant = variant;
+  if (chunk_nnz != P->chunk_nnz || hot_rows != P->hot_rows) {
     P->chunk_nnz = chunk_nnz;
-    int rc = build_chunks(P, st);
+    P->hot_rows = hot_rows;
+    int rc = build_layout(P, st);
     if (rc) return rc;
     rc = rebuild_adjoint_chunks(P, st);
     if (rc) return rc;

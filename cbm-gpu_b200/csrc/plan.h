@@ -15,6 +15,9 @@ struct cbm_plan {
   bool unit_values = true, has_values = false;
   int32_t chunk_nnz = 256;      // split rows longer than this
   int32_t rows_per_claim = 4;   // rows a team takes per queue claim
+  int32_t variant = 0;          // CBM_VARIANT_*: forward kernel choice
+  int64_t hot_rows = 65536;     // columns whose X rows the staged kernel asks L2 to keep (0: no hints)
+  int32_t staged_team = 0;      // lanes per team of the staged kernel (0: its default)
   int64_t launches = 0;
   int64_t last_grid = 0;
   long long timeout_ns = 1000000000ll;  // bounded waits: 1 s
@@ -26,13 +29,18 @@ struct cbm_plan {
   std::vector<int32_t> h_slot;    // internal slot per node (-1: leaf)
   std::vector<int32_t> h_depth;
   std::vector<uint32_t> h_ent;    // column | sign << 31, item order
+  std::vector<float> h_val;       // values in item order (empty when all are +-1)
 
-  // forward layout (device)
+  // forward layout (device); d_ptr/d_ent/d_val and d_cent/d_cval are the
+  // stream layout rebuilt with the chunk size (build_layout)
   int32_t* d_node = nullptr;
   int64_t* d_ptr = nullptr;
   uint32_t* d_ent = nullptr;
   float* d_val = nullptr;
+  uint32_t* d_cent = nullptr;
+  float* d_cval = nullptr;
   int32_t* d_par = nullptr;
+  int32_t* d_par_item = nullptr;
   int32_t* d_self_slot = nullptr;
   int32_t* d_par_slot = nullptr;
   float* d_mult = nullptr;
@@ -69,6 +77,6 @@ struct cbm_plan {
 namespace cbm {
 int cuda_status(cudaError_t e);
 void free_all(std::vector<void*>& v);
-int build_chunks(cbm_plan* P, cudaStream_t st);
+int build_layout(cbm_plan* P, cudaStream_t st);
 int rebuild_adjoint_chunks(cbm_plan* P, cudaStream_t st);
 }  // namespace cbm

@@ -127,10 +127,22 @@ int cbm_plan_create(const int32_t* row_ptr, const int32_t* col_idx, const float*
 /* Copies N multipliers (device pointer) into the plan: D^-1/2 for ADX/DADX. */
 int cbm_plan_set_multipliers(cbm_plan* plan, const float* d_multipliers, void* stream);
 
-/* Re-splits long rows: rows with more than `chunk_nnz` entries are summed in
- * chunks of that size by separate warps (>= 32). rows_per_claim: rows a team
- * takes per queue claim (>= 1).  Host-side re-layout + upload. */
-int cbm_plan_tune(cbm_plan* plan, int32_t chunk_nnz, int32_t rows_per_claim, void* stream);
+/* Tuning knobs.  chunk_nnz (>= 32): rows with more entries are summed in
+ * chunks of that size by separate teams (host-side re-layout + upload).
+ * rows_per_claim (>= 1): consecutive rows a team takes per queue claim.
+ * variant: which forward kernel runs on the 16-byte vector path.
+ * hot_rows (>= 0): the staged kernel asks L2 to keep the X rows of this many
+ * most-gathered columns and to evict the others and the output rows first;
+ * 0 turns the cache policies off.  team (0, 8, 16, 32): lanes per row stream
+ * in the staged kernel (0: its default; several streams share each warp).
+ * Changing chunk_nnz or hot_rows re-lays out the plan (synchronous). */
+enum {
+  CBM_VARIANT_AUTO = 0,     /* staged where it applies, else register gather */
+  CBM_VARIANT_REGISTER = 1, /* X rows gathered into registers, U entries at a time */
+  CBM_VARIANT_STAGED = 2    /* X rows staged through shared memory by cp.async */
+};
+int cbm_plan_tune(cbm_plan* plan, int32_t chunk_nnz, int32_t rows_per_claim, int32_t variant, int64_t hot_rows,
+                  int32_t team, void* stream);
 
 /* Device scratch bytes a call with these operand types needs (0 is possible). */
 int64_t cbm_plan_workspace_bytes(const cbm_plan* plan, int32_t op, int64_t n_cols, int32_t x_dtype,

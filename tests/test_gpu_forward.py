@@ -69,10 +69,12 @@ GRAPHS = {
 @pytest.mark.parametrize("graph", list(GRAPHS))
 @pytest.mark.parametrize("op", ["ax", "adx", "dadx"])
 @pytest.mark.parametrize("cols", [64, 256])
-def test_forward_bit_exact_vs_oracle(graph, op, cols):
+@pytest.mark.parametrize("variant", ["register", "staged"])
+def test_forward_bit_exact_vs_oracle(graph, op, cols, variant):
     dev = _dev()
     ei, n = GRAPHS[graph]()
     a = _make(op, ei, alpha=0)
+    a.plan.tune(variant=variant, rows_per_claim=5)
     assert a.plan.stat(7) == 0, "no row should be split at these sizes"
     g = torch.Generator(device="cpu").manual_seed(0)
     x = (torch.rand(n, cols, generator=g) * 2 - 1).to(dev)
@@ -89,7 +91,8 @@ def test_forward_bit_exact_vs_oracle(graph, op, cols):
 
 
 @pytest.mark.parametrize("op", ["ax", "dadx"])
-def test_split_rows(op):
+@pytest.mark.parametrize("variant", ["register", "staged"])
+def test_split_rows(op, variant):
     """Force chunking (rows longer than 32 entries) and compare to the oracle."""
     dev = _dev()
     from cbm.synthetic import chung_lu_graph, near_duplicates
@@ -97,7 +100,7 @@ def test_split_rows(op):
     rng = np.random.Generator(np.random.PCG64(3))
     ei = near_duplicates(chung_lu_graph(5000, 2.1, 20.0, rng=rng), 5000, 0.3, 0.1, rng=rng)
     a = _make(op, ei, alpha=0)
-    a.plan.tune(chunk_nnz=32, rows_per_claim=2)
+    a.plan.tune(chunk_nnz=32, rows_per_claim=2, variant=variant)
     st = a.plan.stats
     assert st["chunks"] > 0 and st["long_rows"] > 0
     x = torch.randn(5000, 128, device=dev)
@@ -142,11 +145,13 @@ def _abs_sum(op, a, x):
     return s
 
 
-def test_deep_chain():
+@pytest.mark.parametrize("variant", ["register", "staged"])
+def test_deep_chain(variant):
     """A 600-deep chain: every row waits on its parent."""
     dev = _dev()
     ei, n = chain_graph(600)
     a = _make("ax", ei)
+    a.plan.tune(variant=variant)
     assert a.plan.stats["levels"] == 600
     x = torch.randn(n, 32, device=dev)
     y = torch.empty_like(x)
@@ -183,11 +188,13 @@ def test_strided_and_misaligned_views():
 
 
 @pytest.mark.parametrize("ydt", [torch.float32, torch.bfloat16])
-def test_bf16_inputs(ydt):
+@pytest.mark.parametrize("variant", ["register", "staged"])
+def test_bf16_inputs(ydt, variant):
     """BF16 X, FP32 accumulation: equal to the fp32 oracle on the same (bf16) values."""
     dev = _dev()
     ei = near_dup_graph(2500, seed=8)
     a = _make("dadx", ei)
+    a.plan.tune(variant=variant)
     x = torch.randn(2500, 128, device=dev).to(torch.bfloat16)
     y = torch.empty(2500, 128, device=dev, dtype=ydt)
     a.matmul(x, y)
@@ -313,3 +320,20 @@ def test_bounded_wait_times_out_and_recovers():
     a.matmul(x, y)
     assert p.error()[0] == _lib.OK
     np.testing.assert_array_equal(y.cpu().numpy(), _oracle("ax", a, x))
+
+
+@pytest.mark.parametrize("team", [8, 16, 32])
+@pytest.mark.parametrize("cols,dtype", [(256, torch.float32), (64, torch.float32), (128, torch.bfloat16),
+                                        (512, torch.float32)])
+def test_staged_team_shapes(team, cols, dtype):
+    """Every team size of the staged kernel (several row streams per warp stepping
+    together) gives the oracle's result bit for bit on unsplit rows."""
+    dev = _dev()
+    ei = near_dup_graph(3000, seed=23, deg=14)
+    a = _make("dadx", ei)
+    a.plan.tune(variant="staged", team=team, rows_per_claim=3)
+    x = torch.randn(3000, cols, device=dev).to(dtype)
+    y = torch.empty(3000, cols, device=dev)
+    a.matmul(x, y)
+    np.testing.assert_array_equal(y.cpu().numpy(), _oracle("dadx", a, x))
+    a.plan.check_device()
