@@ -320,7 +320,7 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic_from_profile(),
                          "kernel": ("cbm::fwd_kernel<float,float,2,4>" if args.variant == "register"
-                                    else "cbm::fwd_stream_kernel<float,float,2,4,8>"),
+                                    else "cbm::fwd_stream_kernel<float,float,32,2,4,8,128>"),
                          "bytes_alg_per_launch": b_alg},
             "e2e": {"value": b_alg * world / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s",
                     "h2d_bytes_per_step": int(xh.numel() * 4), "d2h_bytes_per_step": int(yh.numel() * 4),
