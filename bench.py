@@ -1,4 +1,5 @@
-"""Benchmark: CBM D^-1/2 A D^-1/2 X throughput (GB/s of algorithmic bytes) on B200.
+"""Benchmark: CBM D^-1/2 A D^-1/2 X throughput (GB/s of algorithmic bytes) on B200,
+and the GCN fwd+bwd time in BF16 against plain FP32.
 
 Workload (default): the 1,000,000-node power-law graph (Chung-Lu exponent 2.1,
 mean degree 20, 30% near-duplicate rows with 10% flips, symmetrised, seed 1),
@@ -7,6 +8,11 @@ D^-1/2 A D^-1/2 X product (cbm4dad.matmul).  X and Y (1.02 GB each) exceed
 the 126 MB L2, so no flush is needed between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+The line also carries "gcn": a 2-layer GCN (128 -> 256 -> 40) on the
+170,000-node power-law graph (exponent 2.1, mean degree 14, 25% near-duplicate
+rows, seed 3), forward + backward ms per step with BF16 activations and with
+plain FP32, and their ratio (rank 0 only).
 
 N > 1 runs under torchrun, one rank per GPU: each rank owns a 256-column shard
 of X and Y (column sharding needs no collective; weak scaling).  Rank 0
@@ -193,6 +199,47 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def gcn_timing(steps, warmup):
+    """2-layer GCN (128 -> 256 -> 40) on the 170,000-node power-law graph: forward +
+    backward ms per step, BF16 activations vs plain FP32 (cbm4dad adjacency)."""
+    from cbm import _lib, synthetic
+    from cbm.cbm4dad import cbm4dad
+    from cbm.gcn import GCN, cross_entropy
+
+    ei, n, spec = synthetic.workload("powerlaw-170k")
+    a = cbm4dad(torch.from_numpy(ei), torch.ones(ei.shape[1]), alpha=spec["alpha"])
+    g = torch.Generator(device="cuda").manual_seed(3)
+    x = torch.randn(n, 128, device="cuda", generator=g)
+    labels = torch.randint(0, 40, (n,), device="cuda", generator=g)
+    out = {"workload": "powerlaw-170k GCN 128-256-40, fwd+bwd, cross-entropy on uniform labels",
+           "nodes": n, "nnz_a": int(a.structure_stats["nnz_a"]), "nnz_delta": int(a.structure_stats["nnz_delta"])}
+    for name, dt in (("bf16", torch.bfloat16), ("fp32", torch.float32)):
+        model = GCN(a, 128, 256, 40, act_dtype=dt)
+        xin = x.to(dt)
+
+        def step():
+            model.w1.grad = None
+            model.w2.grad = None
+            loss = cross_entropy(model(xin), labels)
+            loss.backward()
+
+        for _ in range(warmup):
+            step()
+        torch.cuda.synchronize()
+        l0 = a.plan.stat(_lib.P_LAUNCHES)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+        out[f"{name}_ms"] = e0.elapsed_time(e1) / steps
+        out[f"{name}_cbm_launches_per_step"] = (a.plan.stat(_lib.P_LAUNCHES) - l0) / steps
+    out["speedup_bf16_over_fp32"] = out["fp32_ms"] / out["bf16_ms"]
+    a.plan.check_device()
+    return out
+
+
 def config_dict(n, nnz_a, z, e, b, world):
     return {"workload": f"{WORKLOAD}: D^-1/2 A D^-1/2 X fp32, power-law N={n}, alpha=8, C={COLS} per GPU",
             "nodes": n, "nnz_a": nnz_a, "nnz_delta": z, "tree_edges": e, "branches": b, "cols_per_gpu": COLS,
@@ -206,6 +253,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-gcn", action="store_true")
+    ap.add_argument("--gcn-only", action="store_true", help="only the GCN timing (one JSON object)")
     ap.add_argument("--variant", default="auto", choices=["auto", "register", "staged"])
     ap.add_argument("--chunk-nnz", type=int, default=256)
     ap.add_argument("--rows-per-claim", type=int, default=4)
@@ -231,6 +280,11 @@ def main():
 
     from cbm import _lib
     from cbm.cbm4dad import cbm4dad
+
+    if args.gcn_only:
+        if rank == 0:
+            print(json.dumps(gcn_timing(max(args.steps, 10), max(args.warmup, 3))), flush=True)
+        return
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
@@ -329,6 +383,8 @@ def main():
             "clocks": clk.summary(),
             "plan": a.plan.stats,
         }
+        if not args.no_gcn:
+            line["gcn"] = gcn_timing(max(args.steps, 10), max(args.warmup, 3))
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(a, x.cpu().numpy(), b_alg)
         print(json.dumps(line), flush=True)

@@ -718,6 +718,44 @@ __global__ void __launch_bounds__(BLOCK) fwd_stream_kernel(const FwdArgs a) {
       int cur = 0;  // item (relative) the consumer is in
       float row_dv = __shfl_sync(tmask, m_dv, 0, TL);
       auto next_end = [&]() -> int { return cur < nit ? __shfl_sync(tmask, m_end, cur, TL) : INT_MAX; };
+      // Parent rows are fetched ahead: the parent's ready flag of item i+1 is
+      // acquired when item i starts, and if it was set, item i+1's parent row is
+      // loaded into registers when item i+1 starts; the row end then finds it
+      // there.  A flag not yet set falls back to the bounded wait at the end.
+      bool pf_ok = false;
+      float pbuf[VPL][V];
+      // claims without any parent skip this bookkeeping
+      const bool any_parent = __any_sync(tmask, tl < nit && m_par >= 0);
+      auto acquire_for = [&](int it) -> unsigned {
+        if (!any_parent || it >= nit) return 0u;
+        const int p = __shfl_sync(tmask, m_par, it, TL);
+        return p >= 0 ? ld_acquire(a.node_flag + p) : 0u;
+      };
+      auto prefetch = [&](int it, unsigned fval) {
+        pf_ok = false;
+        if (!any_parent || it >= nit) return;
+        const int p = __shfl_sync(tmask, m_par, it, TL);
+        const int ps = __shfl_sync(tmask, m_pslot, it, TL);
+        if (p < 0 || fval != epoch) return;
+        pf_ok = true;
+#pragma unroll
+        for (int v = 0; v < VPL; ++v) {
+          const int vi = tl + v * TL;
+          if (vi < a.nvec) {
+            if constexpr (sizeof(YT) == 4) {
+              load_y_cg<YT, V>(static_cast<const YT*>(a.y) + (int64_t)p * a.ldy + (int64_t)vi * V, pbuf[v]);
+            } else {
+              load_f32_cg<V>(a.pstate + (int64_t)ps * a.ldp + vi * V, pbuf[v]);
+            }
+          }
+        }
+      };
+      unsigned flag_next;
+      {
+        const unsigned f0 = acquire_for(0);
+        flag_next = acquire_for(1);
+        prefetch(0, f0);
+      }
       auto on_end = [&](float (&acc)[VPL][V]) {
         const int nodew = __shfl_sync(tmask, m_node, cur, TL);
         const int node = nodew & 0x7fffffff;
@@ -743,14 +781,17 @@ __global__ void __launch_bounds__(BLOCK) fwd_stream_kernel(const FwdArgs a) {
             }
           }
         }
-        if (p >= 0 && wait_flag(a.node_flag + p, epoch, a.qs, a.timeout_ns, (long long)node)) {
+        if (p >= 0 && (pf_ok || wait_flag(a.node_flag + p, epoch, a.qs, a.timeout_ns, (long long)node))) {
           const float dp = (a.prop_mode == PROP_RATIO) ? __ldg(a.mult + p) : 1.f;
 #pragma unroll
           for (int v = 0; v < VPL; ++v) {
             const int vi = tl + v * TL;
             if (vi < a.nvec) {
               float yp[V];
-              if constexpr (sizeof(YT) == 4) {
+              if (pf_ok) {
+#pragma unroll
+                for (int q = 0; q < V; ++q) yp[q] = pbuf[v][q];
+              } else if constexpr (sizeof(YT) == 4) {
                 load_y_cg<YT, V>(static_cast<const YT*>(a.y) + (int64_t)p * a.ldy + (int64_t)vi * V, yp);
               } else {
                 load_f32_cg<V>(a.pstate + (int64_t)ps * a.ldp + vi * V, yp);
@@ -797,6 +838,9 @@ __global__ void __launch_bounds__(BLOCK) fwd_stream_kernel(const FwdArgs a) {
           for (int q = 0; q < V; ++q) acc[v][q] = 0.f;
         ++cur;
         row_dv = __shfl_sync(tmask, m_dv, cur < nit ? cur : 0, TL);
+        const unsigned f_cur = flag_next;
+        flag_next = acquire_for(cur + 1);
+        prefetch(cur, f_cur);
       };
       // a parent row inside this warp's claim: let the teams run independently
       const bool lockstep = !__any_sync(0xffffffffu, dep_in_claim);
@@ -817,14 +861,20 @@ constexpr uint32_t kInternalBit = 0x40000000u;
 constexpr uint32_t kIndexMask = 0x3fffffffu;
 
 struct RevArgs {
-  int32_t n_items;       // internal nodes, deepest level first
-  const int32_t* node;
-  const int32_t* slot;
-  const int64_t* ptr;    // children lists
+  // items, deepest level first: for each internal node its chunk items (long
+  // children lists), then the node item
+  int32_t n_items;
+  const int32_t* node;   // node id, or -1 for a chunk item
+  const int32_t* slot;   // node item: internal slot; chunk item: chunk id
+  const int64_t* ptr;    // children (or chunk) ranges in ent
   const uint32_t* ent;   // child | internal bit (slot then)
+  const int32_t* chunk0; // node item: first chunk id, -1 when not split
+  const int32_t* nchunk; // node item: number of chunks
   const float* mult;
   int32_t scale_g;       // G' = m o G
   unsigned int* flag;    // [n_internal]
+  unsigned int* chunk_flag;  // [chunks]
+  float* partial;        // [chunks, ldp]
   QueueState* qs;
   const void* g;
   int64_t ldg;
@@ -883,6 +933,8 @@ __device__ __forceinline__ void gather_dual(float (&acc)[VPL][V], const GT* __re
       const float sgn = (signed_ent && (e >> 31)) ? -1.f : 1.f;
       if (e & kInternalBit) {
         sc = sgn;
+        // each lane acquires the flag of its own entry; the team barrier below
+        // orders every lane's later reads of those rows after these acquires
         if (flag) wait_flag(flag + r, epoch, qs, timeout_ns, (long long)r);
       } else {
         sc = scale_g ? sgn * __ldg(mult + r) : sgn;
@@ -900,10 +952,6 @@ __device__ __forceinline__ void gather_dual(float (&acc)[VPL][V], const GT* __re
         s[u] = __shfl_sync(tmask, sc, src, TL);
         const uint32_t r = eu & kIndexMask;
         const bool in = (eu & kInternalBit) != 0;
-        if (in && flag && j + u < cnt) {
-          // every lane acquires the flag itself before reading the row
-          wait_flag(flag + r, epoch, qs, timeout_ns, (long long)r);
-        }
 #pragma unroll
         for (int v = 0; v < VPL; ++v) {
           const int vi = tl + v * TL;
@@ -954,31 +1002,55 @@ __global__ void __launch_bounds__(kThreads) rev_kernel(const RevArgs a) {
       const int w = a.node[item];
       const int ws = a.slot[item];
       float acc[VPL][V];
-      const float sw = a.scale_g ? __ldg(a.mult + w) : 1.f;
+      if (w >= 0) {
+        // node item: its own G' row
+        const float sw = a.scale_g ? __ldg(a.mult + w) : 1.f;
 #pragma unroll
-      for (int v = 0; v < VPL; ++v) {
-        const int vi = tl + v * TL;
-        if (vi < a.nvec) {
-          float t[V];
-          Vec<GT, V>::load(g + (int64_t)w * a.ldg + (int64_t)vi * V, t);
+        for (int v = 0; v < VPL; ++v) {
+          const int vi = tl + v * TL;
+          if (vi < a.nvec) {
+            float t[V];
+            Vec<GT, V>::load(g + (int64_t)w * a.ldg + (int64_t)vi * V, t);
 #pragma unroll
-          for (int q = 0; q < V; ++q) acc[v][q] = __fmul_rn(sw, t[q]);
-        } else {
+            for (int q = 0; q < V; ++q) acc[v][q] = __fmul_rn(sw, t[q]);
+          } else {
+#pragma unroll
+            for (int q = 0; q < V; ++q) acc[v][q] = 0.f;
+          }
+        }
+        // partial sums of its chunks, in order
+        const int c0 = a.chunk0[item];
+        for (int k = c0, ke = c0 + (c0 >= 0 ? a.nchunk[item] : 0); k < ke; ++k) {
+          if (!wait_flag(a.chunk_flag + k, epoch, a.qs, a.timeout_ns, (long long)k)) continue;
+          const float* prow = a.partial + (int64_t)k * a.ldp;
+#pragma unroll
+          for (int v = 0; v < VPL; ++v) {
+            const int vi = tl + v * TL;
+            if (vi < a.nvec) {
+              float t[V];
+              load_f32_cg<V>(prow + vi * V, t);
+#pragma unroll
+              for (int q = 0; q < V; ++q) acc[v][q] = __fadd_rn(acc[v][q], t[q]);
+            }
+          }
+        }
+      } else {
+#pragma unroll
+        for (int v = 0; v < VPL; ++v)
 #pragma unroll
           for (int q = 0; q < V; ++q) acc[v][q] = 0.f;
-        }
       }
       gather_dual<GT, VPL, V>(acc, g, a.ldg, a.h, a.ldp, a.nvec, a.ent, a.ptr[item], a.ptr[item + 1], a.mult,
                               a.scale_g != 0, false, a.flag, epoch, a.qs, a.timeout_ns, tl, TL, tmask);
-      float* hrow = a.h + (int64_t)ws * a.ldp;
+      float* orow = (w >= 0) ? a.h + (int64_t)ws * a.ldp : a.partial + (int64_t)ws * a.ldp;
 #pragma unroll
       for (int v = 0; v < VPL; ++v) {
         const int vi = tl + v * TL;
-        if (vi < a.nvec) store_f32<V>(hrow + vi * V, acc[v]);
+        if (vi < a.nvec) store_f32<V>(orow + vi * V, acc[v]);
       }
       __threadfence();
       __syncwarp(tmask);
-      if (tl == 0) st_release(a.flag + ws, epoch);
+      if (tl == 0) st_release((w >= 0 ? a.flag : a.chunk_flag) + ws, epoch);
     }
     __syncwarp();
   }
@@ -1058,7 +1130,9 @@ __global__ void __launch_bounds__(kThreads) tr_kernel(const TrArgs a) {
           }
         }
       }
-      const float so = a.scale_out ? __ldg(a.mult + item) : 1.f;
+      // an empty column contributes nothing; do not scale it (m may be inf there)
+      const bool empty = c0 < 0 && a.ptr[item] == a.ptr[item + 1];
+      const float so = (a.scale_out && !empty) ? __ldg(a.mult + item) : 1.f;
       DT* drow = static_cast<DT*>(a.dx) + (int64_t)item * a.lddx;
 #pragma unroll
       for (int v = 0; v < VPL; ++v) {

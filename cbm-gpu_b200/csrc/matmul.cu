@@ -313,21 +313,38 @@ int build_adjoint(cbm_plan* P, cudaStream_t st) {
     for (int64_t v = 0; v < n; ++v)
       if (P->h_parent[v] >= 0) kids[fill[P->h_parent[v]]++] = (int32_t)v;
   }
-  // internal nodes in reverse item (level) order
-  std::vector<int32_t> rnode, rslot;
+  // internal nodes in reverse item (level) order; a children list longer than
+  // kRevChunk is summed in chunk items queued just before its node
+  constexpr int64_t kRevChunk = 64;
+  std::vector<int32_t> rnode, rslot, rchunk0, rnchunk;
   std::vector<int64_t> rptr(1, 0);
   std::vector<uint32_t> rent;
+  int32_t n_rev_chunks = 0;
   for (int64_t i = n - 1; i >= 0; --i) {
     const int32_t w = P->h_order[i];
     if (P->h_slot[w] < 0) continue;
-    rnode.push_back(w);
-    rslot.push_back(P->h_slot[w]);
+    const int64_t nk = cptr[w + 1] - cptr[w];
+    const bool split = nk > kRevChunk;
+    const int32_t first = n_rev_chunks;
     for (int64_t k = cptr[w]; k < cptr[w + 1]; ++k) {
       const int32_t c = kids[k];
       rent.push_back(P->h_slot[c] >= 0 ? ((uint32_t)P->h_slot[c] | kInternalBit) : (uint32_t)c);
+      if (split && ((k - cptr[w] + 1) % kRevChunk == 0 || k + 1 == cptr[w + 1])) {
+        rnode.push_back(-1);  // chunk item
+        rslot.push_back(n_rev_chunks++);
+        rchunk0.push_back(-1);
+        rnchunk.push_back(0);
+        rptr.push_back((int64_t)rent.size());
+      }
     }
-    rptr.push_back((int64_t)rent.size());
+    rnode.push_back(w);
+    rslot.push_back(P->h_slot[w]);
+    rchunk0.push_back(split ? first : -1);
+    rnchunk.push_back(split ? n_rev_chunks - first : 0);
+    rptr.push_back((int64_t)rent.size());  // empty range when split
   }
+  P->n_rev_items = (int64_t)rnode.size();
+  P->n_rev_chunks = n_rev_chunks;
   // transposed delta: column j lists (row v or its slot, sign)
   P->h_t_ptr.assign(P->n_cols + 1, 0);
   for (int64_t k = 0; k < P->nnz; ++k) P->h_t_ptr[(P->h_ent[k] & 0x7fffffffu) + 1]++;
@@ -349,6 +366,9 @@ int build_adjoint(cbm_plan* P, cudaStream_t st) {
   }
   int rc;
   if ((rc = upload(&P->d_rev_node, rnode, st, P->adj_bufs))) return rc;
+  if ((rc = upload(&P->d_rev_chunk0, rchunk0, st, P->adj_bufs))) return rc;
+  if ((rc = upload(&P->d_rev_nchunk, rnchunk, st, P->adj_bufs))) return rc;
+  if ((rc = zeros_u32(&P->d_rev_chunk_flag, n_rev_chunks, st, P->adj_bufs))) return rc;
   if ((rc = upload(&P->d_rev_slot, rslot, st, P->adj_bufs))) return rc;
   if ((rc = upload(&P->d_rev_ptr, rptr, st, P->adj_bufs))) return rc;
   if ((rc = upload(&P->d_rev_ent, rent, st, P->adj_bufs))) return rc;
@@ -377,7 +397,7 @@ int64_t cbm_plan_workspace_bytes(const cbm_plan* P, int32_t op, int64_t n_cols, 
     // chunk counts of the transposed matrix are only known once built; bound
     // them by nnz / chunk_nnz + n_cols
     const int64_t t_chunks = P->adj_built ? P->n_t_chunks : (2 * P->nnz / P->chunk_nnz + 1);
-    rows = P->n_internal + t_chunks;
+    rows = P->n_internal + t_chunks + (P->adj_built ? P->n_rev_chunks : P->n_internal);
   } else {
     rows = P->n_chunks + (y_dtype == CBM_BF16 ? P->n_internal : 0);
   }
@@ -524,19 +544,24 @@ int cbm_matmul_adjoint(cbm_plan* P, int32_t op, const void* g, int32_t gdt, int6
     team_for(nvec, &team, &vpl);
     const int64_t ldp = round4(cols);
     float* h = static_cast<float*>(ws);
-    float* partial = ws ? h + P->n_internal * ldp : nullptr;
+    float* partial = ws ? h + P->n_internal * ldp : nullptr;                 // transposed chunks
+    float* rpartial = ws ? partial + P->n_t_chunks * ldp : nullptr;          // reverse chunks
     const void* gb = static_cast<const char*>(g) + c0 * elem_size(gdt);
     if (P->n_internal > 0) {
       RevArgs r;
       std::memset(&r, 0, sizeof(r));
-      r.n_items = (int32_t)P->n_internal;
+      r.n_items = (int32_t)P->n_rev_items;
       r.node = P->d_rev_node;
       r.slot = P->d_rev_slot;
       r.ptr = P->d_rev_ptr;
       r.ent = P->d_rev_ent;
+      r.chunk0 = P->d_rev_chunk0;
+      r.nchunk = P->d_rev_nchunk;
       r.mult = P->d_mult;
       r.scale_g = op == CBM_OP_DADX;
       r.flag = P->d_adj_flag;
+      r.chunk_flag = P->d_rev_chunk_flag;
+      r.partial = rpartial;
       r.qs = P->d_qs;
       r.g = gb;
       r.ldg = ldg;

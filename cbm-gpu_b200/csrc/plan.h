@@ -56,7 +56,11 @@ struct cbm_plan {
 
   // adjoint layout (built on first use)
   bool adj_built = false;
-  int32_t* d_rev_node = nullptr;   // internal nodes, deepest level first
+  int64_t n_rev_items = 0, n_rev_chunks = 0;
+  int32_t* d_rev_chunk0 = nullptr;
+  int32_t* d_rev_nchunk = nullptr;
+  unsigned* d_rev_chunk_flag = nullptr;
+  int32_t* d_rev_node = nullptr;   // internal nodes (and chunk items), deepest level first
   int32_t* d_rev_slot = nullptr;
   int64_t* d_rev_ptr = nullptr;    // children lists
   uint32_t* d_rev_ent = nullptr;   // child | internal << 30 (slot if internal)

@@ -144,3 +144,34 @@ def test_bf16_gradients():
     ref = _adj_f64("dadx", ei, n, g.float())
     rel = np.abs(x.grad.float().cpu().numpy() - ref).max() / np.abs(ref).max()
     assert rel <= 1e-2, rel
+
+
+def _star_of_copies(n_copies=300, width=31, seed=0):
+    """Row 0 plus n_copies rows that each swap one of its columns: node 0 gets
+    a few hundred children, so its children list is summed in chunks."""
+    rng = np.random.default_rng(seed)
+    n = n_copies + 1 + width + 50
+    base = np.arange(n_copies + 1, n_copies + 1 + width)
+    rows, cols = [], []
+    for r in range(n_copies + 1):
+        c = base.copy()
+        if r > 0:
+            c[rng.integers(0, width)] = n_copies + 1 + width + rng.integers(0, 50)
+        rows += [r] * len(np.unique(c))
+        cols += np.unique(c).tolist()
+    return np.array([rows, cols], dtype=np.int32), n
+
+
+@pytest.mark.parametrize("cols", [40, 256])
+def test_adjoint_many_children(cols):
+    dev = torch.device("cuda")
+    ei, n = _star_of_copies()
+    a = _make("ax", ei)
+    kids = np.bincount(a.mca_src_idx.cpu().numpy(), minlength=n)
+    assert kids.max() > 64, kids.max()
+    g = torch.randn(a.num_nodes, cols, device=dev)
+    dx = torch.empty_like(g)
+    a.adjoint(g, dx)
+    ref = _adj_f64("ax", ei, a.num_nodes, g)
+    assert np.abs(dx.cpu().numpy() - ref).max() <= 1e-4 * np.abs(ref).max()
+    a.plan.check_device()
