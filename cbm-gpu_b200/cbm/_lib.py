@@ -41,7 +41,7 @@ SIGNATURES = [
     ("cbm_plan_create", C.c_int, [vp, vp, vp, i64, i64, i64, vp, i64, vp, vp, i64, vp, i32, vp,
                                   C.POINTER(vp)]),
     ("cbm_plan_set_multipliers", C.c_int, [vp, vp, vp]),
-    ("cbm_plan_tune", C.c_int, [vp, i32, i32, i32, i64, i32, vp]),
+    ("cbm_plan_tune", C.c_int, [vp, i32, i32, i32, i32, i64, i32, vp]),
     ("cbm_plan_workspace_bytes", i64, [vp, i32, i64, i32, i32, i32]),
     ("cbm_matmul", C.c_int, [vp, i32, vp, i32, i64, vp, i32, i64, i64, vp, i64, vp]),
     ("cbm_matmul_adjoint", C.c_int, [vp, i32, vp, i32, i64, vp, i32, i64, i64, vp, i64, vp]),

@@ -102,10 +102,10 @@ class Plan:
                    "cbm_plan_set_multipliers")
         torch.cuda.current_stream(self.device).synchronize()
 
-    def tune(self, chunk_nnz=256, rows_per_claim=4, variant="auto", hot_rows=65536, team=0):
+    def tune(self, chunk_nnz=256, rows_per_claim=4, variant="auto", hot_rows=65536, team=0, rows_per_claim_deep=0):
         v = {"auto": _lib.VARIANT_AUTO, "register": _lib.VARIANT_REGISTER, "staged": _lib.VARIANT_STAGED}[variant]
-        _lib.check(self._lib.cbm_plan_tune(self._h, int(chunk_nnz), int(rows_per_claim), v, int(hot_rows),
-                                           int(team), _stream(self.device)), "cbm_plan_tune")
+        _lib.check(self._lib.cbm_plan_tune(self._h, int(chunk_nnz), int(rows_per_claim), int(rows_per_claim_deep), v,
+                                           int(hot_rows), int(team), _stream(self.device)), "cbm_plan_tune")
         self._ws.clear()
 
     def set_timeout(self, ns):

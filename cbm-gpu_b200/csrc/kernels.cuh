@@ -86,7 +86,9 @@ struct FwdArgs {
   int32_t scale_mode;
   int32_t prop_mode;
   int32_t team;        // lanes per row: 1, 2, 4, 8, 16 or 32
-  int32_t rows_per_claim;
+  int32_t rows_per_claim;       // level-0 rows a team takes per claim
+  int32_t rows_per_claim_deep;  // rows below level 0 a team takes per claim
+  int32_t n_root;               // items [0, n_root) are level 0 (no parent)
   int32_t hints;       // L2 cache policies on (staged kernel)
   long long timeout_ns;
 };
@@ -447,13 +449,17 @@ __global__ void __launch_bounds__(kThreads) fwd_kernel(const FwdArgs a) {
       __syncwarp();
     }
   }
-  const unsigned per_claim = (unsigned)(teams * a.rows_per_claim);
+  // claims of rows_per_claim rows per team while the queue is in level 0, of
+  // rows_per_claim_deep below it (sized by where the warp's last claim fell)
+  unsigned last = 0;
   for (;;) {
+    const int R = last < (unsigned)a.n_root ? a.rows_per_claim : a.rows_per_claim_deep;
     unsigned base = 0;
-    if (lane == 0) base = atomicAdd(&a.qs->next_row, per_claim);
+    if (lane == 0) base = atomicAdd(&a.qs->next_row, (unsigned)(teams * R));
     base = __shfl_sync(0xffffffffu, base, 0);
     if (base >= (unsigned)a.n_items) break;
-    for (int r = 0; r < a.rows_per_claim; ++r) {
+    last = base;
+    for (int r = 0; r < R; ++r) {
       const unsigned item = base + team + (unsigned)(r * teams);
       if (item >= (unsigned)a.n_items) break;
       fwd_row<XT, YT, VPL, V>(a, (int)item, epoch, tl, TL, tmask);
@@ -685,19 +691,24 @@ __global__ void __launch_bounds__(BLOCK) fwd_stream_kernel(const FwdArgs a) {
     }
   }
 
-  // ---- rows: a team takes R consecutive items per claim ----
-  const int R = a.rows_per_claim < TL ? a.rows_per_claim : TL;
-  const unsigned per_claim = (unsigned)(teams * R);
+  // ---- rows: a team takes R consecutive items per claim: rows_per_claim while
+  // the queue is in level 0, rows_per_claim_deep below it (sized by where the
+  // warp's last claim fell)
   const bool need_dv = (a.scale_mode == SCALE_DCOL_DROW) || (a.prop_mode == PROP_RATIO);
+  const int64_t hi = a.n_items;
+  unsigned last = 0;
   for (;;) {
-    unsigned base = 0;
-    if (lane == 0) base = atomicAdd(&a.qs->next_row, per_claim);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (base >= (unsigned)a.n_items) break;
+    const int Rp = last < (unsigned)a.n_root ? a.rows_per_claim : a.rows_per_claim_deep;
+    const int R = Rp < TL ? Rp : TL;
+    unsigned claimed = 0;
+    if (lane == 0) claimed = atomicAdd(&a.qs->next_row, (unsigned)(teams * R));
+    const unsigned base = __shfl_sync(0xffffffffu, claimed, 0);
+    if ((int64_t)base >= hi) break;
+    last = base;
     const int64_t i0 = (int64_t)base + (int64_t)team * R;
     {
-      const int64_t i1 = (i0 + R < a.n_items) ? i0 + R : a.n_items;
-      const int nit = i0 < a.n_items ? (int)(i1 - i0) : 0;
+      const int64_t i1 = (i0 + R < hi) ? i0 + R : hi;
+      const int nit = i0 < hi ? (int)(i1 - i0) : 0;
       const int64_t k0 = nit > 0 ? a.ptr[i0] : 0;
       // item metadata, one item per lane; ends relative to k0
       int m_node = 0, m_par = -1, m_chunk = -1, m_pslot = -1, m_sslot = -1, m_end = 0;

@@ -279,6 +279,8 @@ int cbm_plan_create(const int32_t* row_ptr, const int32_t* col_idx, const float*
   int32_t max_depth = 0;
   for (int64_t v = 0; v < n_rows; ++v) max_depth = std::max(max_depth, depth[v]);
   P->levels = n_rows > 0 ? max_depth + 1 : 0;
+  P->n_root = 0;
+  for (int64_t v = 0; v < n_rows; ++v) P->n_root += depth[v] == 0;
   std::vector<int64_t> lvl_start(max_depth + 2, 0);
   for (int64_t v = 0; v < n_rows; ++v) lvl_start[depth[v] + 1]++;
   for (int32_t l = 0; l <= max_depth; ++l) lvl_start[l + 1] += lvl_start[l];
@@ -379,9 +381,11 @@ int cbm_plan_set_multipliers(cbm_plan* P, const float* d_mult, void* stream) {
   return CBM_OK;
 }
 
-int cbm_plan_tune(cbm_plan* P, int32_t chunk_nnz, int32_t rows_per_claim, int32_t variant, int64_t hot_rows,
-                  int32_t team, void* stream) {
+int cbm_plan_tune(cbm_plan* P, int32_t chunk_nnz, int32_t rows_per_claim, int32_t rows_per_claim_deep,
+                  int32_t variant, int64_t hot_rows, int32_t team, void* stream) {
   if (!P || chunk_nnz < 32 || rows_per_claim < 1 || rows_per_claim > 1024 || hot_rows < 0) return CBM_ERR_INVALID;
+  if (rows_per_claim_deep < 0 || rows_per_claim_deep > 1024) return CBM_ERR_INVALID;
+  P->rows_per_claim_deep = rows_per_claim_deep;
   if (team != 0 && team != 8 && team != 16 && team != 32) return CBM_ERR_INVALID;
   P->staged_team = team;
   if (variant < CBM_VARIANT_AUTO || variant > CBM_VARIANT_STAGED) return CBM_ERR_INVALID;

@@ -14,7 +14,9 @@ struct cbm_plan {
   int64_t n_items = 0, n_internal = 0, levels = 0;
   bool unit_values = true, has_values = false;
   int32_t chunk_nnz = 256;      // split rows longer than this
-  int32_t rows_per_claim = 4;   // rows a team takes per queue claim
+  int32_t rows_per_claim = 4;   // level-0 rows a team takes per queue claim
+  int32_t rows_per_claim_deep = 0;  // rows below level 0 a team takes per claim (0: automatic)
+  int64_t n_root = 0;           // rows at level 0 (children of the virtual root)
   int32_t variant = 0;          // CBM_VARIANT_*: forward kernel choice
   int64_t hot_rows = 65536;     // columns whose X rows the staged kernel asks L2 to keep (0: no hints)
   int32_t staged_team = 0;      // lanes per team of the staged kernel (0: its default)

@@ -129,7 +129,10 @@ int cbm_plan_set_multipliers(cbm_plan* plan, const float* d_multipliers, void* s
 
 /* Tuning knobs.  chunk_nnz (>= 32): rows with more entries are summed in
  * chunks of that size by separate teams (host-side re-layout + upload).
- * rows_per_claim (>= 1): consecutive rows a team takes per queue claim.
+ * rows_per_claim (>= 1): consecutive level-0 rows a team takes per queue
+ * claim; rows_per_claim_deep (>= 0): the same for rows below level 0, which
+ * wait on their parents (0: automatic, one row when more than a quarter of the
+ * rows are below level 0, else rows_per_claim).
  * variant: which forward kernel runs on the 16-byte vector path.
  * hot_rows (>= 0): the staged kernel asks L2 to keep the X rows of this many
  * most-gathered columns and to evict the others and the output rows first;
@@ -141,8 +144,8 @@ enum {
   CBM_VARIANT_REGISTER = 1, /* X rows gathered into registers, U entries at a time */
   CBM_VARIANT_STAGED = 2    /* X rows staged through shared memory by cp.async */
 };
-int cbm_plan_tune(cbm_plan* plan, int32_t chunk_nnz, int32_t rows_per_claim, int32_t variant, int64_t hot_rows,
-                  int32_t team, void* stream);
+int cbm_plan_tune(cbm_plan* plan, int32_t chunk_nnz, int32_t rows_per_claim, int32_t rows_per_claim_deep,
+                  int32_t variant, int64_t hot_rows, int32_t team, void* stream);
 
 /* Device scratch bytes a call with these operand types needs (0 is possible). */
 int64_t cbm_plan_workspace_bytes(const cbm_plan* plan, int32_t op, int64_t n_cols, int32_t x_dtype,
