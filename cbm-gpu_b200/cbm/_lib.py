@@ -21,6 +21,7 @@ OP_AX, OP_ADX, OP_DADX, OP_VALUES_ADD, OP_VALUES_RATIO, OP_DAD_ADD = range(6)
 INPUT_DEVICE, INPUT_HOST = 0, 1
 VARIANT_AUTO, VARIANT_REGISTER, VARIANT_STAGED = 0, 1, 2
 BUILD_EXHAUSTIVE = 1
+COALESCE_SYMMETRIZE, COALESCE_DROP_SELF = 1, 2
 S_DELTA_ROW, S_DELTA_COL, S_DELTA_VAL, S_BRANCHES, S_SRC, S_DST, S_PARENT, S_CSR_PTR, S_CSR_COL, \
     S_CSR_VAL = range(10)
 S_N_CANDIDATES, S_TREE_COST, S_NNZ_A = 100, 101, 102
@@ -34,6 +35,7 @@ i64 = C.c_int64
 # (name, restype, argtypes): every exported symbol of include/cbm_b200.h
 SIGNATURES = [
     ("cbm_build", C.c_int, [vp, vp, i64, i64, i64, i32, i32, C.POINTER(vp)]),
+    ("cbm_coalesce", C.c_int, [vp, vp, i64, i64, i32, vp, vp, C.POINTER(i64)]),
     ("cbm_structure_len", i64, [vp, i32]),
     ("cbm_structure_copy", C.c_int, [vp, i32, vp]),
     ("cbm_structure_free", None, [vp]),

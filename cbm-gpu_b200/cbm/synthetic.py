@@ -40,17 +40,31 @@ def _rng(seed):
     return np.random.Generator(np.random.PCG64(seed))
 
 
+def coalesce_csr(rows, cols, n, symmetrize=True, drop_self=True):
+    """COO -> CSR (int64 ptr, int32 sorted unique columns) by the library's
+    native coalescer (cbm_coalesce)."""
+    import ctypes as C
+
+    from . import _lib
+
+    lib = _lib.load()
+    r = np.ascontiguousarray(rows, dtype=np.int32)
+    c = np.ascontiguousarray(cols, dtype=np.int32)
+    ptr = np.empty(n + 1, dtype=np.int64)
+    out = np.empty(max(1, r.size * (2 if symmetrize else 1)), dtype=np.int32)
+    nnz = C.c_int64(0)
+    flags = (_lib.COALESCE_SYMMETRIZE if symmetrize else 0) | (_lib.COALESCE_DROP_SELF if drop_self else 0)
+    _lib.check(lib.cbm_coalesce(r.ctypes.data, c.ctypes.data, r.size, n, flags, ptr.ctypes.data, out.ctypes.data,
+                                C.byref(nnz)), "cbm_coalesce")
+    return ptr, out[: nnz.value]
+
+
 def coalesce_symmetric(rows, cols, n):
     """A | A^T with self-loops removed; returns int32 [2, nnz] sorted by (row, col)."""
-    rows = np.asarray(rows, dtype=np.int64)
-    cols = np.asarray(cols, dtype=np.int64)
-    keep = rows != cols
-    rows, cols = rows[keep], cols[keep]
-    key = np.concatenate([rows * n + cols, cols * n + rows])
-    key = np.unique(key)
-    out = np.empty((2, key.size), dtype=np.int32)
-    out[0] = key // n
-    out[1] = key % n
+    ptr, col = coalesce_csr(rows, cols, n)
+    out = np.empty((2, col.size), dtype=np.int32)
+    out[0] = np.repeat(np.arange(n, dtype=np.int32), np.diff(ptr))
+    out[1] = col
     return out
 
 

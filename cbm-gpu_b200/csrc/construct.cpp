@@ -633,6 +633,48 @@ int cbm_build(const int32_t* row, const int32_t* col, int64_t nnz, int64_t n_row
   return CBM_OK;
 }
 
+int cbm_coalesce(const int32_t* row, const int32_t* col, int64_t nnz, int64_t n, int32_t flags, int64_t* ptr,
+                 int32_t* out_col, int64_t* out_nnz) {
+  if (!ptr || !out_nnz || n < 0 || nnz < 0 || (nnz > 0 && (!row || !col || !out_col))) return CBM_ERR_INVALID;
+  const bool sym = flags & CBM_COALESCE_SYMMETRIZE;
+  const bool drop = flags & CBM_COALESCE_DROP_SELF;
+  for (int64_t k = 0; k < nnz; ++k)
+    if (row[k] < 0 || row[k] >= n || col[k] < 0 || col[k] >= n) return CBM_ERR_INDEX;
+  try {
+    std::vector<int64_t> cnt(n + 1, 0);
+    for (int64_t k = 0; k < nnz; ++k) {
+      if (drop && row[k] == col[k]) continue;
+      cnt[row[k] + 1]++;
+      if (sym && row[k] != col[k]) cnt[col[k] + 1]++;
+    }
+    for (int64_t i = 0; i < n; ++i) cnt[i + 1] += cnt[i];
+    std::vector<int64_t> fill(cnt.begin(), cnt.end() - 1);
+    for (int64_t k = 0; k < nnz; ++k) {
+      if (drop && row[k] == col[k]) continue;
+      out_col[fill[row[k]]++] = col[k];
+      if (sym && row[k] != col[k]) out_col[fill[col[k]]++] = row[k];
+    }
+    std::vector<int64_t> len(n, 0);
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (int64_t i = 0; i < n; ++i) {
+      int32_t* b = out_col + cnt[i];
+      int32_t* e = out_col + cnt[i + 1];
+      std::sort(b, e);
+      len[i] = std::unique(b, e) - b;
+    }
+    // compact in place (rows move left only)
+    ptr[0] = 0;
+    for (int64_t i = 0; i < n; ++i) {
+      if (ptr[i] != cnt[i] && len[i] > 0) std::memmove(out_col + ptr[i], out_col + cnt[i], len[i] * sizeof(int32_t));
+      ptr[i + 1] = ptr[i] + len[i];
+    }
+    *out_nnz = ptr[n];
+  } catch (const std::bad_alloc&) {
+    return CBM_ERR_ALLOC;
+  }
+  return CBM_OK;
+}
+
 int64_t cbm_structure_len(const cbm_structure* s, int32_t which) {
   if (!s) return -1;
   switch (which) {

@@ -75,6 +75,15 @@ enum { CBM_BUILD_EXHAUSTIVE = 1 }; /* every pair sharing a column (for checks) *
 int cbm_build(const int32_t* row, const int32_t* col, int64_t nnz, int64_t n_rows, int64_t alpha,
               int32_t n_threads, int32_t flags, cbm_structure** out);
 
+/* COO -> CSR with sorted, unique columns per row, the canonical form the
+ * constructor works on (the reference's mkl_sparse_convert_csr,
+ * cbm/cbm_extensions.cpp:70-98).  flags: CBM_COALESCE_SYMMETRIZE adds every
+ * edge's transpose, CBM_COALESCE_DROP_SELF drops (i, i).  ptr: int64 [n+1];
+ * out_col: capacity nnz (2 nnz with SYMMETRIZE).  Host, OpenMP. */
+enum { CBM_COALESCE_SYMMETRIZE = 1, CBM_COALESCE_DROP_SELF = 2 };
+int cbm_coalesce(const int32_t* row, const int32_t* col, int64_t nnz, int64_t n, int32_t flags, int64_t* ptr,
+                 int32_t* out_col, int64_t* out_nnz);
+
 /* The six arrays cbm_init_ returns (cbm/cbm_extensions.cpp:301-344), in its
  * order, then extras: the delta matrix as CSR (rows sorted, one block per row),
  * the parent of each node (N = virtual root), and counters. */
