@@ -240,6 +240,88 @@ def gcn_timing(steps, warmup):
     return out
 
 
+def _time_events(fn, steps, warmup):
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def run_batch(args):
+    """Batching form: 512 community graphs (log-uniform 1,000..64,000 nodes, mean
+    degree U[8, 40], seed 4) in one launch replayed from a CUDA graph;
+    D^-1/2 A D^-1/2 X with X [sum N, 64] BF16, Y FP32; autotuned."""
+    from cbm import _lib, synthetic
+    from cbm.batch import cbm_batch
+    from cbm.tune import autotune
+
+    t0 = time.time()
+    graphs = synthetic.batch_graphs(512, seed=4)
+    b = cbm_batch(graphs, alpha=0, op="dadx")
+    setup_s = time.time() - t0
+    n = b.num_nodes
+    g = torch.Generator(device="cuda").manual_seed(4)
+    x = torch.randn(n, 64, device="cuda", generator=g).to(torch.bfloat16)
+    y = torch.empty(n, 64, device="cuda")
+    tuned = autotune(b.plan, "dadx", x, y, space={"chunk_nnz": [128, 256], "rows_per_claim": [2, 4, 8],
+                                                  "variant": ["auto", "register"]})
+    graph = b.capture(x, y)
+    l0 = b.plan.stat(_lib.P_LAUNCHES)
+    ms = _time_events(graph.replay, args.steps, args.warmup)
+    st = b.plan.stats
+    b_alg = bytes_alg(n, st["nnz"], st["edges"], st["branches"], 64, sx=2, sy=4)
+    line = {"metric": "CBM batched DAD.X GB/s (algorithmic bytes)", "value": b_alg / (ms * 1e-3) / 1e9,
+            "unit": "GB/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "dtype": "bf16 X, f32 Y, f32 accumulate", "data": "synthetic",
+            "config": {"workload": "512 community graphs, one launch under a CUDA graph", "graphs": len(graphs),
+                       "nodes": n, "nnz_a": b.nnz_a, "nnz_delta": st["nnz"], "tree_edges": st["edges"],
+                       "cols": 64, "setup_s": setup_s},
+            "graphs_per_s": len(graphs) / (ms * 1e-3), "rows_per_s": n / (ms * 1e-3),
+            "launches_per_step": (b.plan.stat(_lib.P_LAUNCHES) - l0) / args.steps,
+            "autotune_best": {"config": tuned[0][0], "ms": tuned[0][1]},
+            "roofline": {"bound": "hbm", "achieved": b_alg / (ms * 1e-3) / 1e9, "peak": peaks()[0], "unit": "GB/s",
+                         "frac": b_alg / (ms * 1e-3) / 1e9 / peaks()[0], "peak_kind": peaks()[1]}}
+    b.plan.check_device()
+    print(json.dumps(line), flush=True)
+
+
+def run_precision(args):
+    """Precision form: A D^-1/2 X on the 2,400,000-node power-law graph
+    (exponent 2.3, mean degree 50, 40% near-duplicate rows with 5% flips, seed 2,
+    alpha 16); X [N, 128] stored BF16, FP32 accumulation and output."""
+    from cbm import _lib, synthetic
+    from cbm.cbm4ad import cbm4ad
+
+    t0 = time.time()
+    ei, n, spec = synthetic.workload("powerlaw-2.4m")
+    a = cbm4ad(torch.from_numpy(ei), torch.ones(ei.shape[1]), alpha=spec["alpha"])
+    setup_s = time.time() - t0
+    g = torch.Generator(device="cuda").manual_seed(2)
+    x = torch.randn(n, 128, device="cuda", generator=g).to(torch.bfloat16)
+    y = torch.empty(n, 128, device="cuda")
+    ms = _time_events(lambda: a.matmul(x, y), args.steps, args.warmup)
+    st = a.plan.stats
+    b_alg = bytes_alg(n, st["nnz"], st["edges"], st["branches"], 128, sx=2, sy=4)
+    line = {"metric": "CBM A.D^-1/2.X GB/s (algorithmic bytes), BF16 X", "value": b_alg / (ms * 1e-3) / 1e9,
+            "unit": "GB/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "dtype": "bf16 X, f32 Y, f32 accumulate", "data": "synthetic",
+            "config": {"workload": "powerlaw-2.4m A D^-1/2 X", "nodes": n,
+                       "nnz_a": a.structure_stats["nnz_a"], "nnz_delta": st["nnz"], "tree_edges": st["edges"],
+                       "cols": 128, "alpha": spec["alpha"], "setup_s": setup_s},
+            "rows_per_s": n / (ms * 1e-3),
+            "roofline": {"bound": "hbm", "achieved": b_alg / (ms * 1e-3) / 1e9, "peak": peaks()[0], "unit": "GB/s",
+                         "frac": b_alg / (ms * 1e-3) / 1e9 / peaks()[0], "peak_kind": peaks()[1]},
+            "plan": st}
+    a.plan.check_device()
+    print(json.dumps(line), flush=True)
+
+
 def config_dict(n, nnz_a, z, e, b, world):
     return {"workload": f"{WORKLOAD}: D^-1/2 A D^-1/2 X fp32, power-law N={n}, alpha=8, C={COLS} per GPU",
             "nodes": n, "nnz_a": nnz_a, "nnz_delta": z, "tree_edges": e, "branches": b, "cols_per_gpu": COLS,
@@ -255,6 +337,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-gcn", action="store_true")
     ap.add_argument("--gcn-only", action="store_true", help="only the GCN timing (one JSON object)")
+    ap.add_argument("--workload", default="headline", choices=["headline", "batch", "precision"],
+                    help="batch / precision: the batching or precision form instead of the headline line")
     ap.add_argument("--variant", default="auto", choices=["auto", "register", "staged"])
     ap.add_argument("--chunk-nnz", type=int, default=256)
     ap.add_argument("--rows-per-claim", type=int, default=4)
@@ -281,6 +365,10 @@ def main():
     from cbm import _lib
     from cbm.cbm4dad import cbm4dad
 
+    if args.workload != "headline":
+        if rank == 0:
+            (run_batch if args.workload == "batch" else run_precision)(args)
+        return
     if args.gcn_only:
         if rank == 0:
             print(json.dumps(gcn_timing(max(args.steps, 10), max(args.warmup, 3))), flush=True)
