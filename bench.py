@@ -270,7 +270,7 @@ def run_batch(args):
     x = torch.randn(n, 64, device="cuda", generator=g).to(torch.bfloat16)
     y = torch.empty(n, 64, device="cuda")
     tuned = autotune(b.plan, "dadx", x, y, space={"chunk_nnz": [128, 256], "rows_per_claim": [2, 4, 8],
-                                                  "variant": ["auto", "register"]})
+                                                  "variant": ["auto", "register"], "team": [0, 8]})
     graph = b.capture(x, y)
     l0 = b.plan.stat(_lib.P_LAUNCHES)
     ms = _time_events(graph.replay, args.steps, args.warmup)
@@ -301,6 +301,8 @@ def run_precision(args):
     t0 = time.time()
     ei, n, spec = synthetic.workload("powerlaw-2.4m")
     a = cbm4ad(torch.from_numpy(ei), torch.ones(ei.shape[1]), alpha=spec["alpha"])
+    a.plan.tune(chunk_nnz=args.chunk_nnz, rows_per_claim=args.rows_per_claim, variant=args.variant,
+                hot_rows=args.hot_rows, team=args.team)
     setup_s = time.time() - t0
     g = torch.Generator(device="cuda").manual_seed(2)
     x = torch.randn(n, 128, device="cuda", generator=g).to(torch.bfloat16)

@@ -532,7 +532,8 @@ __device__ __forceinline__ float entry_scale(uint32_t e, int64_t idx, bool valid
 // Positions are 32-bit and relative to k0; batches of TL entries start at
 // multiples of TL.  next_end() gives the relative position where the
 // current item ends (INT_MAX when none is left); on_end(acc) finishes it,
-// resets acc and advances, updating row_dv (the row factor of SCALE_DCOL_DROW).
+// resets acc and advances, updating row_dv (the row factor: m[row] under
+// SCALE_DCOL_DROW, exactly 1 otherwise).
 template <typename XT, int TL, int VPL, int V, int S, int BLOCK, typename NextEnd, typename OnEnd>
 __device__ __forceinline__ void stream_pass(const XT* __restrict__ x, int64_t ldx, int nvec,
                                             const uint32_t* __restrict__ ent, const float* __restrict__ val,
@@ -595,9 +596,11 @@ __device__ __forceinline__ void stream_pass(const XT* __restrict__ x, int64_t ld
   // Only when no team waits on a row another team of the warp produces in the
   // same pass (the caller checks): a wait would then block the producer at
   // the per-step warp barrier.
-  const int wlen = lockstep ? __reduce_max_sync(0xffffffffu, len) : len;
+  // (a full-warp team is alone in its warp: no lockstep, every step active)
+  const bool ls = TL < 32 && lockstep;
+  const int wlen = ls ? __reduce_max_sync(0xffffffffu, len) : len;
   for (int k = 0; k < wlen; ++k) {
-    const bool active = k < len;
+    const bool active = TL == 32 || k < len;
     if (active) {
       while (k == end_at) {
         on_end(acc);
@@ -615,8 +618,8 @@ __device__ __forceinline__ void stream_pass(const XT* __restrict__ x, int64_t ld
       eC = ic < len ? __ldcs(ent0 + ic) : 0u;
     }
     cp_async_wait<S - 1>();
-    float sc = __shfl_sync(tmask, sA, k & (TL - 1), TL);
-    if (scale_mode == SCALE_DCOL_DROW) sc = __fmul_rn(sc, row_dv);
+    // row_dv is m[row] under SCALE_DCOL_DROW and exactly 1 otherwise
+    float sc = __fmul_rn(__shfl_sync(tmask, sA, k & (TL - 1), TL), row_dv);
     if (!active) sc = 0.f;
     uint4* sp = my + slot * (VPL * BLOCK);
 #pragma unroll
@@ -630,14 +633,14 @@ __device__ __forceinline__ void stream_pass(const XT* __restrict__ x, int64_t ld
     }
     produce(k + S, sp);
     slot = (slot + 1 == S) ? 0 : slot + 1;
-    if (lockstep) __syncwarp();
+    if (ls) __syncwarp();
   }
   cp_async_wait<0>();
   while (end_at <= len) {
     on_end(acc);
     end_at = next_end();
   }
-  if (lockstep) __syncwarp();
+  if (ls) __syncwarp();
 }
 
 template <typename XT, typename YT, int TL, int VPL, int V, int S, int BLOCK>
@@ -727,7 +730,8 @@ __global__ void __launch_bounds__(BLOCK) fwd_stream_kernel(const FwdArgs a) {
       }
       const int len = nit > 0 ? __shfl_sync(tmask, m_end, nit - 1, TL) : 0;
       int cur = 0;  // item (relative) the consumer is in
-      float row_dv = __shfl_sync(tmask, m_dv, 0, TL);
+      const bool drow = a.scale_mode == SCALE_DCOL_DROW;
+      float row_dv = drow ? __shfl_sync(tmask, m_dv, 0, TL) : 1.f;
       auto next_end = [&]() -> int { return cur < nit ? __shfl_sync(tmask, m_end, cur, TL) : INT_MAX; };
       // Parent rows are fetched ahead: the parent's ready flag of item i+1 is
       // acquired when item i starts, and if it was set, item i+1's parent row is
@@ -774,7 +778,7 @@ __global__ void __launch_bounds__(BLOCK) fwd_stream_kernel(const FwdArgs a) {
         const int p = __shfl_sync(tmask, m_par, cur, TL);
         const int ps = __shfl_sync(tmask, m_pslot, cur, TL);
         const int ss = __shfl_sync(tmask, m_sslot, cur, TL);
-        const float dv = row_dv;
+        const float dv = __shfl_sync(tmask, m_dv, cur, TL);
         if (c0 >= 0) {
           const int item = (int)(i0 + cur);
           for (int k = c0; k < a.n_chunks && a.chunk_item[k] == item; ++k) {
@@ -848,7 +852,8 @@ __global__ void __launch_bounds__(BLOCK) fwd_stream_kernel(const FwdArgs a) {
 #pragma unroll
           for (int q = 0; q < V; ++q) acc[v][q] = 0.f;
         ++cur;
-        row_dv = __shfl_sync(tmask, m_dv, cur < nit ? cur : 0, TL);
+        const float next_dv = __shfl_sync(tmask, m_dv, cur < nit ? cur : 0, TL);
+        row_dv = drow ? next_dv : 1.f;
         const unsigned f_cur = flag_next;
         flag_next = acquire_for(cur + 1);
         prefetch(cur, f_cur);
