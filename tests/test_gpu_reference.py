@@ -135,12 +135,28 @@ def test_time_reference_vs_ours(ref_mod):
     t_ref = timeit(lambda: ref.matmul_DAX_DADX(x, y1))
     t_ours = timeit(lambda: ours.matmul(x, y2))
     torch.testing.assert_close(y2, y1, rtol=RTOL, atol=ATOL)
+    # the reference's CSR baseline (cbm/csr.cu) on D^-1/2 A D^-1/2 itself
+    from oracle import build_ref, oracle
+
+    csr_mod = build_ref.load("csr_cusparse_ref")
+    t_csr = None
+    if csr_mod is not None:
+        ptr, idx = oracle.csr_from_edges(ei, n)
+        rows = torch.repeat_interleave(torch.arange(n, device=dev), torch.from_numpy(np.diff(ptr)).to(dev))
+        colt = torch.from_numpy(idx).to(dev)
+        vals = ours.D[rows] * ours.D[colt.long()]
+        ahat = torch.sparse_csr_tensor(torch.from_numpy(ptr.astype(np.int32)).to(dev), colt, vals, (n, n))
+        csr = csr_mod.cusparseCSR(ahat)
+        y3 = torch.empty_like(x)
+        t_csr = timeit(lambda: csr.matmul(x, y3))
+        torch.testing.assert_close(y3, y1, rtol=1e-4, atol=1e-5)
     st = ours.plan.stats
     from bench import bytes_alg
 
     b = bytes_alg(n, st["nnz"], st["edges"], st["branches"], 256)
     rec = {"workload": "powerlaw-1m dadx C=256", "ref_ms": t_ref, "ours_ms": t_ours, "ref_gbs": b / t_ref / 1e6,
-           "ours_gbs": b / t_ours / 1e6, "speedup": t_ref / t_ours, "when": time.time()}
+           "ours_gbs": b / t_ours / 1e6, "speedup": t_ref / t_ours, "ref_csr_ms": t_csr,
+           "speedup_vs_csr": (t_csr / t_ours) if t_csr else None, "when": time.time()}
     print("REFTIMING", json.dumps(rec))
     os.makedirs("gpurun_out", exist_ok=True)
     with open("gpurun_out/ref_timing.json", "w") as f:
