@@ -60,20 +60,57 @@ def bytes_alg(n, z, e, b, cols, sx=4, sy=4, scaled=True):
 
 
 def load_graph(rank, world):
-    """Edge list + CBM structure, built once and shared through a file cache."""
-    from cbm import cbm_mkl_cpp, synthetic
+    """Edge list of the workload, generated once by rank 0 into a file cache that
+    every rank reads after a barrier."""
+    from cbm import synthetic
+    from cbm.shard import build_once
 
     cache = os.path.join(REPO, "_cache")
     os.makedirs(cache, exist_ok=True)
-    path = os.path.join(cache, f"{WORKLOAD}.npz")
-    if rank == 0 and not os.path.exists(path):
-        ei, n, spec = synthetic.workload(WORKLOAD)
-        np.savez(path + ".tmp.npz", ei=ei, n=n)
-        os.replace(path + ".tmp.npz", path)
-    if world > 1:
-        torch.distributed.barrier()
-    d = np.load(path)
+
+    def make(path):
+        ei, n, _ = synthetic.workload(WORKLOAD)
+        with open(path, "wb") as f:
+            np.savez(f, ei=ei, n=n)
+
+    d = np.load(build_once(os.path.join(cache, f"{WORKLOAD}.npz"), make, rank))
     return d["ei"], int(d["n"]), synthetic.WORKLOADS[WORKLOAD]
+
+
+def fp64_sample_error(ei, n, x, y, rs=None, cs=None, rows=4096, seed=0):
+    """Max-abs and relative error of y = rs o (A (cs o x)) on a sample of rows
+    against FP64 sums over the original A (the edge list, not the CBM form)."""
+    r = np.asarray(ei[0])
+    c = np.asarray(ei[1])
+    ptr = np.zeros(n + 1, dtype=np.int64)
+    ptr[1:] = np.cumsum(np.bincount(r, minlength=n))
+    order = np.argsort(r, kind="stable") if np.any(np.diff(r) < 0) else None
+    cols = c[order] if order is not None else c
+    pick = np.sort(np.random.default_rng(seed).choice(n, size=min(rows, n), replace=False))
+    lens = ptr[pick + 1] - ptr[pick]
+    nb = np.concatenate([cols[ptr[v]:ptr[v + 1]] for v in pick]).astype(np.int64)
+    xs = x[torch.from_numpy(nb).to(x.device)].double().cpu().numpy()
+    if cs is not None:
+        xs *= cs[nb][:, None]
+    starts = np.concatenate([[0], np.cumsum(lens)[:-1]])
+    ref = np.zeros((pick.size, xs.shape[1]))
+    has = lens > 0
+    ref[has] = np.add.reduceat(xs, starts[has], axis=0)
+    if rs is not None:
+        ref *= rs[pick][:, None]
+    out = y[torch.from_numpy(pick).to(y.device)].double().cpu().numpy()
+    diff = np.abs(out - ref)
+    return {"rows_sampled": int(pick.size), "max_abs": float(diff.max()),
+            "max_rel": float(diff.max() / max(np.abs(ref).max(), 1e-300)),
+            "rel_fro": float(np.linalg.norm(out - ref) / max(np.linalg.norm(ref), 1e-300))}
+
+
+def dinv_f64(ei, n):
+    deg = np.bincount(np.asarray(ei[0]), minlength=n).astype(np.float64)
+    with np.errstate(divide="ignore"):
+        d = 1.0 / np.sqrt(deg)
+    d[deg == 0] = 0.0
+    return d
 
 
 class Clocks:
@@ -287,6 +324,11 @@ def run_batch(args):
             "autotune_best": {"config": tuned[0][0], "ms": tuned[0][1]},
             "roofline": {"bound": "hbm", "achieved": b_alg / (ms * 1e-3) / 1e9, "peak": peaks()[0], "unit": "GB/s",
                          "frac": b_alg / (ms * 1e-3) / 1e9 / peaks()[0], "peak_kind": peaks()[1]}}
+    offs = b.offsets
+    packed = np.concatenate([np.asarray(ei, dtype=np.int64) + int(offs[i]) for i, (ei, _) in enumerate(graphs)],
+                            axis=1)
+    dinv = dinv_f64(packed, n)
+    line["error_vs_fp64"] = fp64_sample_error(packed, n, x, y, rs=dinv, cs=dinv)
     b.plan.check_device()
     print(json.dumps(line), flush=True)
 
@@ -305,9 +347,13 @@ def run_precision(args):
                 hot_rows=args.hot_rows, team=args.team)
     setup_s = time.time() - t0
     g = torch.Generator(device="cuda").manual_seed(2)
-    x = torch.randn(n, 128, device="cuda", generator=g).to(torch.bfloat16)
+    x32 = torch.randn(n, 128, device="cuda", generator=g)
+    x = x32.to(torch.bfloat16)
     y = torch.empty(n, 128, device="cuda")
     ms = _time_events(lambda: a.matmul(x, y), args.steps, args.warmup)
+    dinv = dinv_f64(ei, n)
+    err = {"product": fp64_sample_error(ei, n, x, y, cs=dinv),
+           "end_to_end": fp64_sample_error(ei, n, x32, y, cs=dinv)}
     st = a.plan.stats
     b_alg = bytes_alg(n, st["nnz"], st["edges"], st["branches"], 128, sx=2, sy=4)
     line = {"metric": "CBM A.D^-1/2.X GB/s (algorithmic bytes), BF16 X", "value": b_alg / (ms * 1e-3) / 1e9,
@@ -319,7 +365,8 @@ def run_precision(args):
             "rows_per_s": n / (ms * 1e-3),
             "roofline": {"bound": "hbm", "achieved": b_alg / (ms * 1e-3) / 1e9, "peak": peaks()[0], "unit": "GB/s",
                          "frac": b_alg / (ms * 1e-3) / 1e9 / peaks()[0], "peak_kind": peaks()[1]},
-            "plan": st}
+            "plan": st,
+            "error_vs_fp64": err}
     a.plan.check_device()
     print(json.dumps(line), flush=True)
 
@@ -376,9 +423,14 @@ def main():
             print(json.dumps(gcn_timing(max(args.steps, 10), max(args.warmup, 3))), flush=True)
         return
 
+    from cbm.shard import column_shard, max_over_ranks
+
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     ei, n, spec = load_graph(rank, world)
+    # weak scaling: rank r owns columns [c0, c1) of a [N, COLS * world] X and Y
+    c0, c1 = column_shard(COLS * world, rank, world)
+    assert c1 - c0 == COLS
     a = cbm4dad(torch.from_numpy(ei), torch.ones(ei.shape[1]), alpha=spec["alpha"])
     a.plan.tune(chunk_nnz=args.chunk_nnz, rows_per_claim=args.rows_per_claim, variant=args.variant,
                 hot_rows=args.hot_rows, team=args.team)
@@ -412,11 +464,9 @@ def main():
     launches = a.plan.stat(_lib.P_LAUNCHES) - launches0
     per = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
     ms = evs[0].elapsed_time(evs[-1]) / args.steps
-    ms_all = torch.tensor([ms], device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(ms_all, op=torch.distributed.ReduceOp.MAX)
-    ms_max = float(ms_all.item())
+    ms_max = max_over_ranks(ms, dev)
     a.plan.check_device()
+    err = fp64_sample_error(ei, n, x, y, rs=dinv_f64(ei, n), cs=dinv_f64(ei, n)) if rank == 0 else None
 
     # ---- end to end through the public API with host buffers ----
     xh = torch.empty(n, COLS, dtype=torch.float32, pin_memory=True)
@@ -437,15 +487,13 @@ def main():
         yh.copy_(y, non_blocking=True)
     e1.record(stream)
     barrier()
-    e2e_ms = torch.tensor([e0.elapsed_time(e1) / e2e_steps], device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(e2e_ms, op=torch.distributed.ReduceOp.MAX)
-    e2e_ms = float(e2e_ms.item())
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / e2e_steps, dev)
 
     if rank == 0:
         peak, peak_kind = peaks()
         kernel_ms = statistics.mean(per)
         achieved = b_alg / (kernel_ms * 1e-3) / 1e9
+        traffic = traffic_from_profile()
         line = {
             "metric": "CBM DAD.X GB/s (algorithmic bytes)",
             "value": b_alg * world / (ms_max * 1e-3) / 1e9,
@@ -462,7 +510,9 @@ def main():
             "config": config_dict(n, a.structure_stats["nnz_a"], z, e, b, world),
             "rows_per_s": n * world / (ms_max * 1e-3),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic_from_profile(),
+                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+                         "dram_achieved": traffic / (kernel_ms * 1e-3) / 1e9 if traffic else None,
+                         "dram_frac": traffic / (kernel_ms * 1e-3) / 1e9 / peak if traffic else None,
                          "kernel": ("cbm::fwd_kernel<float,float,2,4>" if args.variant == "register"
                                     else "cbm::fwd_stream_kernel<float,float,32,2,4,8,128>"),
                          "bytes_alg_per_launch": b_alg},
@@ -472,6 +522,7 @@ def main():
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
             "plan": a.plan.stats,
+            "error_vs_fp64": err,
         }
         if not args.no_gcn:
             line["gcn"] = gcn_timing(max(args.steps, 10), max(args.warmup, 3))
