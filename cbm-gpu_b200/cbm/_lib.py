@@ -47,6 +47,7 @@ SIGNATURES = [
     ("cbm_plan_workspace_bytes", i64, [vp, i32, i64, i32, i32, i32]),
     ("cbm_matmul", C.c_int, [vp, i32, vp, i32, i64, vp, i32, i64, i64, vp, i64, vp]),
     ("cbm_matmul_adjoint", C.c_int, [vp, i32, vp, i32, i64, vp, i32, i64, i64, vp, i64, vp]),
+    ("cbm_matmul_host", C.c_int, [vp, i32, vp, i32, i64, vp, i32, i64, i64, i64, vp, vp, vp, i64, vp]),
     ("cbm_plan_prepare_adjoint", C.c_int, [vp, vp]),
     ("cbm_plan_set_timeout", C.c_int, [vp, i64]),
     ("cbm_plan_debug_set_parent", C.c_int, [vp, i64, i32, vp]),

@@ -51,6 +51,12 @@ class cbm4mm:  # noqa: N801 (the reference's class name)
     def matmul(self, x, y):
         self._plan.matmul(self._op, x, y)
 
+    def matmul_host(self, x, y, slab_cols=64):
+        """y <- (this operator) x for host tensors x and y (pinned for full-speed
+        copies), the copies overlapped with the product slab by slab.  Queued on
+        the current stream: synchronise it before reading y."""
+        self._plan.matmul_host(self._op, x, y, slab_cols)
+
     def adjoint(self, g, dx):
         """dx <- (this operator)^T g."""
         self._plan.adjoint(self._op, g, dx)

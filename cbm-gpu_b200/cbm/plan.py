@@ -164,6 +164,38 @@ class Plan:
                                   ws.data_ptr(), ws.numel(), _stream(self.device))
         _lib.check(rc, "cbm_matmul")
 
+    def matmul_host(self, op, x, y, slab_cols=64):
+        """y <- op(A) x with x and y in host memory (pinned for full-speed copies):
+        column slabs are copied in, multiplied and copied out on overlapping
+        streams.  Device buffers of the operand shapes are allocated on the first
+        call and reused.  Returns once queued; the current stream waits for the
+        last copy (synchronise it before reading y)."""
+        op = OPS[op] if isinstance(op, str) else int(op)
+        for t, rows, name in ((x, self.n_cols, "rhs"), (y, self.n_rows, "res")):
+            if not isinstance(t, torch.Tensor) or t.is_cuda:
+                raise RuntimeError(f"{name}: expected a host (CPU) tensor")
+            if t.dtype not in _DT:
+                raise RuntimeError(f"{name}: dtype {t.dtype} is not supported (float32 or bfloat16)")
+            if t.dim() != 2 or t.shape[0] != rows or (t.shape[1] > 1 and t.stride(1) != 1):
+                raise RuntimeError(f"{name}: expected a row-major [{rows}, C] tensor")
+        if x.shape[1] != y.shape[1]:
+            raise RuntimeError(f"rhs has {x.shape[1]} columns, res {y.shape[1]}")
+        cols = int(x.shape[1])
+        xdt, ydt = _DT[x.dtype], _DT[y.dtype]
+        key = (cols, x.dtype, y.dtype)
+        bufs = getattr(self, "_host_bufs", {})
+        if key not in bufs:
+            bufs.clear()
+            bufs[key] = (torch.empty(self.n_cols, cols, dtype=x.dtype, device=self.device),
+                         torch.empty(self.n_rows, cols, dtype=y.dtype, device=self.device))
+            self._host_bufs = bufs
+        xd, yd = bufs[key]
+        ws = self.workspace(op, cols, xdt, ydt, False)  # covers every slab width
+        rc = self._lib.cbm_matmul_host(self._h, op, x.data_ptr(), xdt, max(int(x.stride(0)), cols, 1), y.data_ptr(),
+                                       ydt, max(int(y.stride(0)), cols, 1), cols, int(slab_cols), xd.data_ptr(),
+                                       yd.data_ptr(), ws.data_ptr(), ws.numel(), _stream(self.device))
+        _lib.check(rc, "cbm_matmul_host")
+
     def adjoint(self, op, g, dx):
         """dx <- op(A)^T g on the current stream."""
         op = OPS[op] if isinstance(op, str) else int(op)

@@ -73,6 +73,11 @@ bool dtype_ok(int32_t xdt, int32_t ydt) {
          (xdt == CBM_BF16 && ydt == CBM_BF16);
 }
 
+// bytes from the first to one past the last element of a [rows, cols] view with leading dimension ld
+int64_t extent(int64_t rows, int64_t ld, int64_t cols, int32_t dt) {
+  return rows > 0 ? ((rows - 1) * ld + cols) * elem_size(dt) : 0;
+}
+
 bool overlaps(const void* a, int64_t abytes, const void* b, int64_t bbytes) {
   const uintptr_t a0 = reinterpret_cast<uintptr_t>(a), b0 = reinterpret_cast<uintptr_t>(b);
   return a0 < b0 + (uintptr_t)bbytes && b0 < a0 + (uintptr_t)abytes;
@@ -379,6 +384,26 @@ int build_adjoint(cbm_plan* P, cudaStream_t st) {
   return rebuild_adjoint_chunks(P, st);
 }
 
+void release_pipeline(cbm_plan* P) {
+  for (cudaEvent_t e : P->events) cudaEventDestroy(e);
+  P->events.clear();
+  if (P->h2d) cudaStreamDestroy(P->h2d);
+  if (P->d2h) cudaStreamDestroy(P->d2h);
+  P->h2d = P->d2h = nullptr;
+}
+
+// Copy streams (created on the plan's device) and at least `n` events.
+int pipeline_ready(cbm_plan* P, size_t n) {
+  if (!P->h2d && cudaStreamCreateWithFlags(&P->h2d, cudaStreamNonBlocking) != cudaSuccess) return CBM_ERR_CUDA;
+  if (!P->d2h && cudaStreamCreateWithFlags(&P->d2h, cudaStreamNonBlocking) != cudaSuccess) return CBM_ERR_CUDA;
+  while (P->events.size() < n) {
+    cudaEvent_t e;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return CBM_ERR_CUDA;
+    P->events.push_back(e);
+  }
+  return CBM_OK;
+}
+
 }  // namespace cbm
 
 using namespace cbm;
@@ -435,7 +460,7 @@ int cbm_matmul(cbm_plan* P, int32_t op, const void* x, int32_t xdt, int64_t ldx,
   if (n_cols == 0 || P->n_rows == 0) return CBM_OK;
   if (!x || !y) return CBM_ERR_INVALID;
   if (ldx < n_cols || ldy < n_cols) return CBM_ERR_SHAPE;
-  if (overlaps(x, P->n_cols * ldx * elem_size(xdt), y, P->n_rows * ldy * elem_size(ydt))) return CBM_ERR_SHAPE;
+  if (overlaps(x, extent(P->n_cols, ldx, n_cols, xdt), y, extent(P->n_rows, ldy, n_cols, ydt))) return CBM_ERR_SHAPE;
   const bool needs_mult = op == CBM_OP_ADX || op == CBM_OP_DADX || op == CBM_OP_VALUES_RATIO || op == CBM_OP_DAD_ADD;
   if (needs_mult && (!P->d_mult || P->n_rows != P->n_cols)) return CBM_ERR_UNSUPPORTED;
   if ((op == CBM_OP_VALUES_ADD || op == CBM_OP_VALUES_RATIO) && xdt != CBM_F32) return CBM_ERR_DTYPE;
@@ -522,6 +547,69 @@ int cbm_matmul(cbm_plan* P, int32_t op, const void* x, int32_t xdt, int64_t ldx,
   return CBM_OK;
 }
 
+int cbm_matmul_host(cbm_plan* P, int32_t op, const void* x_host, int32_t xdt, int64_t ldx_host, void* y_host,
+                    int32_t ydt, int64_t ldy_host, int64_t n_cols, int64_t slab_cols, void* x_dev, void* y_dev,
+                    void* ws, int64_t ws_bytes, void* stream) {
+  if (!P || n_cols < 0 || slab_cols < 0) return CBM_ERR_INVALID;
+  if (!dtype_ok(xdt, ydt)) return CBM_ERR_DTYPE;
+  if (n_cols == 0 || P->n_rows == 0) return CBM_OK;
+  if (!x_host || !y_host || !x_dev || !y_dev) return CBM_ERR_INVALID;
+  if (ldx_host < n_cols || ldy_host < n_cols) return CBM_ERR_SHAPE;
+  const int64_t xs = elem_size(xdt), ys = elem_size(ydt);
+  // slabs: a multiple of 16 bytes wide in both operands where possible
+  int64_t w = slab_cols == 0 ? n_cols : std::min(slab_cols, n_cols);
+  const int64_t unit = 16 / std::min(xs, ys);
+  if (w < n_cols && w % unit != 0) w = std::min(n_cols, (w + unit - 1) / unit * unit);
+  // slab boundaries: the first and the last slab are half as wide (rounded to
+  // the 16-byte unit), since the copy-in of the first and the copy-out of the
+  // last overlap nothing; the others are w wide
+  std::vector<int64_t> bounds(1, 0);
+  const int64_t h = std::max(unit, (w / 2 + unit - 1) / unit * unit);
+  if (w < n_cols && n_cols >= w + 2 * h) {
+    bounds.push_back(h);
+    while (n_cols - bounds.back() > w + h) bounds.push_back(bounds.back() + w);
+    if (n_cols - bounds.back() > h) bounds.push_back(n_cols - h);
+  } else {
+    while (n_cols - bounds.back() > w) bounds.push_back(bounds.back() + w);
+  }
+  bounds.push_back(n_cols);
+  const int64_t n_slabs = (int64_t)bounds.size() - 1;
+  if (n_slabs > 4096) return CBM_ERR_INVALID;
+  // the product's own checks (workspace, multipliers, op) run on the first slab
+  int rc = pipeline_ready(P, (size_t)(2 * n_slabs + 2));
+  if (rc) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaEvent_t* ev = P->events.data();
+  // the copy streams start after the work already queued on the caller's stream
+  if (cudaEventRecord(ev[0], st) != cudaSuccess) return CBM_ERR_CUDA;
+  if (cudaStreamWaitEvent(P->h2d, ev[0], 0) != cudaSuccess) return CBM_ERR_CUDA;
+  if (cudaStreamWaitEvent(P->d2h, ev[0], 0) != cudaSuccess) return CBM_ERR_CUDA;
+  const char* xh = static_cast<const char*>(x_host);
+  char* yh = static_cast<char*>(y_host);
+  char* xd = static_cast<char*>(x_dev);
+  char* yd = static_cast<char*>(y_dev);
+  for (int64_t k = 0; k < n_slabs; ++k) {
+    const int64_t c0 = bounds[k], cw = bounds[k + 1] - c0;
+    cudaEvent_t in = ev[2 + 2 * k], out = ev[3 + 2 * k];
+    if (cudaMemcpy2DAsync(xd + c0 * xs, n_cols * xs, xh + c0 * xs, ldx_host * xs, cw * xs, P->n_cols,
+                          cudaMemcpyHostToDevice, P->h2d) != cudaSuccess)
+      return CBM_ERR_CUDA;
+    if (cudaEventRecord(in, P->h2d) != cudaSuccess) return CBM_ERR_CUDA;
+    if (cudaStreamWaitEvent(st, in, 0) != cudaSuccess) return CBM_ERR_CUDA;
+    rc = cbm_matmul(P, op, xd + c0 * xs, xdt, n_cols, yd + c0 * ys, ydt, n_cols, cw, ws, ws_bytes, stream);
+    if (rc) return rc;
+    if (cudaEventRecord(out, st) != cudaSuccess) return CBM_ERR_CUDA;
+    if (cudaStreamWaitEvent(P->d2h, out, 0) != cudaSuccess) return CBM_ERR_CUDA;
+    if (cudaMemcpy2DAsync(yh + c0 * ys, ldy_host * ys, yd + c0 * ys, n_cols * ys, cw * ys, P->n_rows,
+                          cudaMemcpyDeviceToHost, P->d2h) != cudaSuccess)
+      return CBM_ERR_CUDA;
+  }
+  // the caller's stream resumes once the last slab is back in host memory
+  if (cudaEventRecord(ev[1], P->d2h) != cudaSuccess) return CBM_ERR_CUDA;
+  if (cudaStreamWaitEvent(st, ev[1], 0) != cudaSuccess) return CBM_ERR_CUDA;
+  return CBM_OK;
+}
+
 int cbm_plan_prepare_adjoint(cbm_plan* P, void* stream) {
   if (!P) return CBM_ERR_INVALID;
   return build_adjoint(P, static_cast<cudaStream_t>(stream));
@@ -534,7 +622,7 @@ int cbm_matmul_adjoint(cbm_plan* P, int32_t op, const void* g, int32_t gdt, int6
   if (n_cols == 0 || P->n_rows == 0 || P->n_cols == 0) return CBM_OK;
   if (!g || !dx) return CBM_ERR_INVALID;
   if (ldg < n_cols || lddx < n_cols) return CBM_ERR_SHAPE;
-  if (overlaps(g, P->n_rows * ldg * elem_size(gdt), dx, P->n_cols * lddx * elem_size(ddt))) return CBM_ERR_SHAPE;
+  if (overlaps(g, extent(P->n_rows, ldg, n_cols, gdt), dx, extent(P->n_cols, lddx, n_cols, ddt))) return CBM_ERR_SHAPE;
   if ((op == CBM_OP_ADX || op == CBM_OP_DADX) && (!P->d_mult || P->n_rows != P->n_cols)) return CBM_ERR_UNSUPPORTED;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   int rc = build_adjoint(P, st);

@@ -444,6 +444,7 @@ void cbm_plan_destroy(cbm_plan* P) {
   int cur = -1;
   cudaGetDevice(&cur);
   if (cur != P->device) cudaSetDevice(P->device);
+  release_pipeline(P);
   free_all(P->chunk_bufs);
   free_all(P->adj_bufs);
   free_all(P->adj_chunk_bufs);

@@ -78,6 +78,11 @@ struct cbm_plan {
   unsigned* d_t_chunk_flag = nullptr;
 
   std::vector<void*> bufs, chunk_bufs, adj_bufs, adj_chunk_bufs;
+
+  // host-operand pipeline (cbm_matmul_host): two copy streams and the events
+  // that order slabs across them, created on first use
+  cudaStream_t h2d = nullptr, d2h = nullptr;
+  std::vector<cudaEvent_t> events;
 };
 
 namespace cbm {
@@ -85,4 +90,5 @@ int cuda_status(cudaError_t e);
 void free_all(std::vector<void*>& v);
 int build_layout(cbm_plan* P, cudaStream_t st);
 int rebuild_adjoint_chunks(cbm_plan* P, cudaStream_t st);
+void release_pipeline(cbm_plan* P);
 }  // namespace cbm

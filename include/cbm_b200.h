@@ -170,6 +170,22 @@ int cbm_matmul(cbm_plan* plan, int32_t op, const void* x, int32_t x_dtype, int64
                int32_t y_dtype, int64_t ldy, int64_t n_cols, void* workspace, int64_t workspace_bytes,
                void* stream);
 
+/* Y = op(A) X for operands in host memory (page-locked for full-speed
+ * copies): X is copied in and Y out in column slabs of slab_cols columns (0:
+ * one slab), with the host-to-device copy of slab k+1, the product of slab k
+ * and the device-to-host copy of slab k-1 overlapped on two copy streams of
+ * the plan and `stream`.  x_host [n_cols(A), n_cols] with leading dimension
+ * ldx_host, y_host [n_rows(A), n_cols] with ldy_host; x_dev / y_dev: device
+ * buffers of the same shapes, contiguous (the caller's: nothing is
+ * allocated); workspace as for cbm_matmul with slab_cols columns.  Returns
+ * once everything is queued; `stream` waits for the last copy, so a
+ * synchronisation of `stream` makes y_host final.  Calls on one plan must be
+ * ordered on one stream.  The reference has no host-operand product (its
+ * callers copy with torch before matmul_AX_ADX, cbm/cbm4mm.py:53-54). */
+int cbm_matmul_host(cbm_plan* plan, int32_t op, const void* x_host, int32_t x_dtype, int64_t ldx_host,
+                    void* y_host, int32_t y_dtype, int64_t ldy_host, int64_t n_cols, int64_t slab_cols,
+                    void* x_dev, void* y_dev, void* workspace, int64_t workspace_bytes, void* stream);
+
 /* dX = op(A)^T G (the adjoint of cbm_matmul for CBM_OP_AX/ADX/DADX): a
  * reverse tree propagation (children into parents) then a transposed delta
  * gather.  Same conventions as cbm_matmul.  No counterpart in the reference. */
