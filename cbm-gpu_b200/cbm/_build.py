@@ -2,7 +2,7 @@
 
     python -m cbm._build            (from cbm-gpu_b200/)
 
-Sources: cbm-gpu_b200/csrc/{construct.cpp, plan.cu, matmul.cu}; header include/.
+Sources: cbm-gpu_b200/csrc/{construct.cpp, plan.cu, matmul.cu, noalloc.cu, transpose.cu}; header include/.
 Objects go to cbm-gpu_b200/_build/, the library next to this file.
 """
 from __future__ import annotations
@@ -22,7 +22,7 @@ BUILD = os.path.join(PKG_ROOT, "_build")
 LIB = os.path.join(HERE, "libcbm_b200.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["construct.cpp", "plan.cu", "matmul.cu", "noalloc.cu"]
+SOURCES = ["construct.cpp", "plan.cu", "matmul.cu", "noalloc.cu", "transpose.cu"]
 HEADERS = ["kernels.cuh", "plan.h"]
 
 

@@ -50,7 +50,9 @@ SIGNATURES = [
     ("cbm_matmul_host", C.c_int, [vp, i32, vp, i32, i64, vp, i32, i64, i64, i64, vp, vp, vp, i64, vp]),
     ("cbm_plan_prepare_adjoint", C.c_int, [vp, vp]),
     ("cbm_plan_set_timeout", C.c_int, [vp, i64]),
+    ("cbm_plan_set_compensation", C.c_int, [vp, i32]),
     ("cbm_plan_debug_set_parent", C.c_int, [vp, i64, i32, vp]),
+    ("cbm_plan_debug_check_transpose", C.c_int, [vp, vp]),
     ("cbm_plan_error", C.c_int, [vp, vp, C.POINTER(i32), C.POINTER(i64)]),
     ("cbm_matmul_noalloc", C.c_int, [vp, vp, vp, i64, i64, vp, vp, i64, vp, vp, vp, i64, vp, vp]),
     ("cbm_plan_stat", i64, [vp, i32]),

@@ -108,6 +108,11 @@ class Plan:
                                            int(hot_rows), int(team), _stream(self.device)), "cbm_plan_tune")
         self._ws.clear()
 
+    def set_compensation(self, min_depth):
+        """BF16 X: compensated propagation from tree depth ``min_depth`` on (-1: off)."""
+        _lib.check(self._lib.cbm_plan_set_compensation(self._h, int(min_depth)), "cbm_plan_set_compensation")
+        self._ws.clear()
+
     def set_timeout(self, ns):
         _lib.check(self._lib.cbm_plan_set_timeout(self._h, int(ns)), "cbm_plan_set_timeout")
 

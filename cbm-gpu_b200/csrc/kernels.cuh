@@ -90,6 +90,13 @@ struct FwdArgs {
   int32_t rows_per_claim_deep;  // rows below level 0 a team takes per claim
   int32_t n_root;               // items [0, n_root) are level 0 (no parent)
   int32_t hints;       // L2 cache policies on (staged kernel)
+  // compensated propagation (register kernel, COMP = true): items from
+  // comp_item0 on (tree depth >= the plan's threshold) add their parent term
+  // with an error-free sum and carry the rounding residual; items from
+  // comp_read0 on (depth >= threshold + 1) read their parent's residual row
+  int32_t comp_item0;
+  int32_t comp_read0;
+  float* pcomp;        // [n_internal, ldp] residual rows of internal nodes
   long long timeout_ns;
 };
 
@@ -335,7 +342,14 @@ __device__ __forceinline__ void fwd_chunk(const FwdArgs& a, int k, unsigned epoc
   if (tl == 0) st_release(a.chunk_flag + k, epoch);
 }
 
-template <typename XT, typename YT, int VPL, int V>
+// s + e == a + b exactly (Knuth's TwoSum; explicit roundings, no contraction)
+__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
+  s = __fadd_rn(a, b);
+  const float bp = __fsub_rn(s, a);
+  e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bp)), __fsub_rn(b, bp));
+}
+
+template <typename XT, typename YT, int VPL, int V, bool COMP = false>
 __device__ __forceinline__ void fwd_row(const FwdArgs& a, int item, unsigned epoch, int tl, int TL, unsigned tmask) {
   float acc[VPL][V];
 #pragma unroll
@@ -368,6 +382,14 @@ __device__ __forceinline__ void fwd_row(const FwdArgs& a, int item, unsigned epo
     }
   }
   const int p = a.par[item];
+  // compensated arithmetic for this row, a residual to read from the parent
+  const bool cmode = COMP && item >= a.comp_item0;
+  const bool cread = COMP && item >= a.comp_read0;
+  float cres[VPL][V];  // unused (and removed by the compiler) without COMP
+#pragma unroll
+  for (int v = 0; v < VPL; ++v)
+#pragma unroll
+    for (int q = 0; q < V; ++q) cres[v][q] = 0.f;
   // after a failed (timed-out) wait the parent is left out; the error is recorded
   if (p >= 0 && wait_flag(a.node_flag + p, epoch, a.qs, a.timeout_ns, (long long)node)) {
     const float dp = (a.prop_mode == PROP_RATIO) ? __ldg(a.mult + p) : 1.f;
@@ -382,13 +404,59 @@ __device__ __forceinline__ void fwd_row(const FwdArgs& a, int item, unsigned epo
         } else {
           load_f32_cg<V>(a.pstate + (int64_t)ps * a.ldp + vi * V, yp);
         }
-        if (a.prop_mode == PROP_RATIO) {
+        if (COMP && cmode) {
+          // parent value = yp + rp (rp: its residual); add with TwoSum and keep
+          // the rounding errors (of the ratio's product and quotient too)
+          float rp[V];
+          if (cread) {
+            load_f32_cg<V>(a.pcomp + (int64_t)ps * a.ldp + vi * V, rp);
+          } else {
+#pragma unroll
+            for (int q = 0; q < V; ++q) rp[q] = 0.f;
+          }
+#pragma unroll
+          for (int q = 0; q < V; ++q) {
+            float t = yp[q], r = rp[q];
+            if (a.prop_mode == PROP_RATIO) {
+              const float prod = __fmul_rn(yp[q], dv);
+              const float pe = fmaf(yp[q], dv, -prod);     // prod + pe == yp * dv
+              t = __fdiv_rn(prod, dp);
+              const float qe = __fdiv_rn(fmaf(-t, dp, prod), dp);  // t + qe ~ prod / dp
+              r = __fadd_rn(__fdiv_rn(fmaf(r, dv, pe), dp), qe);
+            }
+            float s_, e_;
+            two_sum(acc[v][q], t, s_, e_);
+            acc[v][q] = s_;
+            cres[v][q] = __fadd_rn(r, e_);
+          }
+        } else if (a.prop_mode == PROP_RATIO) {
 #pragma unroll
           for (int q = 0; q < V; ++q) acc[v][q] = __fadd_rn(acc[v][q], __fdiv_rn(__fmul_rn(yp[q], dv), dp));
         } else {
 #pragma unroll
           for (int q = 0; q < V; ++q) acc[v][q] = __fadd_rn(acc[v][q], yp[q]);
         }
+      }
+    }
+  }
+  if (COMP && cmode) {
+    // the row's value is acc + cres, rounded once; its residual is kept for
+    // the children of an internal node
+#pragma unroll
+    for (int v = 0; v < VPL; ++v)
+#pragma unroll
+      for (int q = 0; q < V; ++q) {
+        float s_, e_;
+        two_sum(acc[v][q], cres[v][q], s_, e_);
+        acc[v][q] = s_;
+        cres[v][q] = e_;
+      }
+    if (internal) {
+      float* crow = a.pcomp + (int64_t)a.self_slot[item] * a.ldp;
+#pragma unroll
+      for (int v = 0; v < VPL; ++v) {
+        const int vi = tl + v * TL;
+        if (vi < a.nvec) store_f32<V>(crow + vi * V, cres[v]);
       }
     }
   }
@@ -428,7 +496,7 @@ __device__ __forceinline__ void finish_block(QueueState* qs, unsigned epoch) {
   }
 }
 
-template <typename XT, typename YT, int VPL, int V>
+template <typename XT, typename YT, int VPL, int V, bool COMP = false>
 __global__ void __launch_bounds__(kThreads) fwd_kernel(const FwdArgs a) {
   const int lane = threadIdx.x & 31;
   const int TL = a.team;
@@ -462,7 +530,7 @@ __global__ void __launch_bounds__(kThreads) fwd_kernel(const FwdArgs a) {
     for (int r = 0; r < R; ++r) {
       const unsigned item = base + team + (unsigned)(r * teams);
       if (item >= (unsigned)a.n_items) break;
-      fwd_row<XT, YT, VPL, V>(a, (int)item, epoch, tl, TL, tmask);
+      fwd_row<XT, YT, VPL, V, COMP>(a, (int)item, epoch, tl, TL, tmask);
     }
     __syncwarp();
   }
@@ -489,6 +557,14 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
 __device__ __forceinline__ void cp_async16_hint(void* smem, const void* gmem, uint64_t policy) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;" ::"r"(s), "l"(gmem), "l"(policy)
+               : "memory");
+}
+// copies `bytes` (16 or 0) and zero-fills the rest: a copy that may be empty
+// without a branch (the address must still point into the operand)
+__device__ __forceinline__ void cp_async16_hint_n(void* smem, const void* gmem, unsigned bytes, uint64_t policy) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2, %3;" ::"r"(s), "l"(gmem), "r"(bytes),
+               "l"(policy)
                : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
@@ -569,8 +645,20 @@ __device__ __forceinline__ void stream_pass(const XT* __restrict__ x, int64_t ld
     sA = entry_scale(eA, ia, ia < len, scale_mode, mult, val0);
     sB = entry_scale(eB, ib, ib < len, scale_mode, mult, val0);
   }
+  // entry p's pieces into ring slot sp (no commit).  One piece per lane
+  // (narrow rows): branch-free, a piece outside the row or an entry past the
+  // stream's end (its word is 0, so the address is X's first row) copies 0
+  // bytes and zero-fills the slot.  Several pieces per lane: pieces outside
+  // the row and entries past the end are skipped (the slots keep old data,
+  // never read).
   auto produce = [&](int p, uint4* sp) {
-    if (p < len) {
+    if constexpr (VPL == 1) {
+      const bool inA = p < bA + TL;
+      const uint32_t e = __shfl_sync(tmask, inA ? eA : eB, p & (TL - 1), TL);
+      const XT* row = xl + (int64_t)(e & kColMask) * ldx;
+      const uint64_t pol = (e & kHotBit) ? pol_keep : pol_stream;
+      cp_async16_hint_n(sp, piece_ok[0] ? row : x, (p < len && piece_ok[0]) ? 16u : 0u, pol);
+    } else if (p < len) {
       const bool inA = p < bA + TL;
       const uint32_t e = __shfl_sync(tmask, inA ? eA : eB, p & (TL - 1), TL);
       const XT* row = xl + (int64_t)(e & kColMask) * ldx;
@@ -579,10 +667,19 @@ __device__ __forceinline__ void stream_pass(const XT* __restrict__ x, int64_t ld
       for (int v = 0; v < VPL; ++v)
         if (piece_ok[v]) cp_async16_hint(sp + v * BLOCK, row + v * TL * V, pol);
     }
-    cp_async_commit();
   };
+  // Entries move in groups of U (one cp.async group each, S / U groups in
+  // flight); a group without a row end inside is consumed by straight-line
+  // code (all U scales, then all U pieces, then the FMAs), one with a row end
+  // (or past the stream's end) entry by entry.
+  constexpr int U = S >= 8 ? 4 : 2;
+  constexpr int G = S / U;
+  static_assert(S % U == 0 && TL % U == 0, "groups must tile the ring and the batches");
 #pragma unroll
-  for (int j = 0; j < S; ++j) produce(j, my + j * (VPL * BLOCK));
+  for (int j = 0; j < S; ++j) {
+    produce(j, my + j * (VPL * BLOCK));
+    if (j % U == U - 1) cp_async_commit();
+  }
 
   float acc[VPL][V];
 #pragma unroll
@@ -590,7 +687,7 @@ __device__ __forceinline__ void stream_pass(const XT* __restrict__ x, int64_t ld
 #pragma unroll
     for (int q = 0; q < V; ++q) acc[v][q] = 0.f;
   int end_at = next_end();
-  int slot = 0;
+  int slot = 0;  // ring slot of entry k (a multiple of U)
   // With lockstep, all teams of the warp step together (to the warp's longest
   // stream) so that one instruction serves every team, finished teams idling.
   // Only when no team waits on a row another team of the warp produces in the
@@ -599,14 +696,19 @@ __device__ __forceinline__ void stream_pass(const XT* __restrict__ x, int64_t ld
   // (a full-warp team is alone in its warp: no lockstep, every step active)
   const bool ls = TL < 32 && lockstep;
   const int wlen = ls ? __reduce_max_sync(0xffffffffu, len) : len;
-  for (int k = 0; k < wlen; ++k) {
-    const bool active = TL == 32 || k < len;
-    if (active) {
-      while (k == end_at) {
-        on_end(acc);
-        end_at = next_end();
+  auto consume = [&](int kk, uint4* sp, bool active) {
+    float sc = __fmul_rn(__shfl_sync(tmask, sA, kk & (TL - 1), TL), row_dv);
+#pragma unroll
+    for (int v = 0; v < VPL; ++v) {
+      if (piece_ok[v] && active) {
+        float t[V];
+        unpack16<XT, V>(sp[v * BLOCK], t);
+#pragma unroll
+        for (int q = 0; q < V; ++q) acc[v][q] = fmaf(sc, t[q], acc[v][q]);
       }
     }
+  };
+  for (int k = 0; k < wlen; k += U) {
     if (k == bA + TL) {
       // rotate: A <- B (scales ready), B <- C (scales now), load a new C
       bA += TL;
@@ -617,22 +719,47 @@ __device__ __forceinline__ void stream_pass(const XT* __restrict__ x, int64_t ld
       sB = entry_scale(eB, ib, ib < len, scale_mode, mult, val0);
       eC = ic < len ? __ldcs(ent0 + ic) : 0u;
     }
-    cp_async_wait<S - 1>();
-    // row_dv is m[row] under SCALE_DCOL_DROW and exactly 1 otherwise
-    float sc = __fmul_rn(__shfl_sync(tmask, sA, k & (TL - 1), TL), row_dv);
-    if (!active) sc = 0.f;
+    cp_async_wait<G - 1>();
     uint4* sp = my + slot * (VPL * BLOCK);
+    if (k + U <= len && end_at >= k + U) {
+      // row_dv is m[row] under SCALE_DCOL_DROW and exactly 1 otherwise
+      if constexpr (VPL == 1) {
+        // all U scales, then all U pieces, then the FMAs (the zero-filled
+        // pieces of lanes outside the row add zeros to unused accumulators)
+        float sc[U];
+        uint4 raw[U];
 #pragma unroll
-    for (int v = 0; v < VPL; ++v) {
-      if (piece_ok[v] && active) {
-        float t[V];
-        unpack16<XT, V>(sp[v * BLOCK], t);
+        for (int u = 0; u < U; ++u) sc[u] = __fmul_rn(__shfl_sync(tmask, sA, (k + u) & (TL - 1), TL), row_dv);
 #pragma unroll
-        for (int q = 0; q < V; ++q) acc[v][q] = fmaf(sc, t[q], acc[v][q]);
+        for (int u = 0; u < U; ++u) raw[u] = sp[u * BLOCK];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          float t[V];
+          unpack16<XT, V>(raw[u], t);
+#pragma unroll
+          for (int q = 0; q < V; ++q) acc[0][q] = fmaf(sc[u], t[q], acc[0][q]);
+        }
+      } else {
+#pragma unroll
+        for (int u = 0; u < U; ++u) consume(k + u, sp + u * (VPL * BLOCK), true);
+      }
+    } else {
+      for (int u = 0; u < U; ++u) {
+        const int kk = k + u;
+        const bool active = kk < len;
+        if (active) {
+          while (kk == end_at) {
+            on_end(acc);
+            end_at = next_end();
+          }
+        }
+        consume(kk, sp + u * (VPL * BLOCK), active);
       }
     }
-    produce(k + S, sp);
-    slot = (slot + 1 == S) ? 0 : slot + 1;
+#pragma unroll
+    for (int u = 0; u < U; ++u) produce(k + S + u, sp + u * (VPL * BLOCK));
+    cp_async_commit();
+    slot = (slot + U == S) ? 0 : slot + U;
     if (ls) __syncwarp();
   }
   cp_async_wait<0>();

@@ -30,6 +30,11 @@ int grid_for(K kernel, int device) {
 }
 
 int64_t round4(int64_t x) { return (x + 3) / 4 * 4; }
+
+// compensated propagation applies to BF16 X on trees deeper than the threshold
+bool comp_active(const cbm_plan* P, int32_t xdt) {
+  return xdt == CBM_BF16 && P->comp_depth >= 0 && P->levels > P->comp_depth && P->n_internal > 0;
+}
 int64_t align256(int64_t b) { return (b + 255) / 256 * 256; }
 
 // Columns one launch covers: 32 lanes x 8 vectors x V elements.
@@ -84,14 +89,14 @@ bool overlaps(const void* a, int64_t abytes, const void* b, int64_t bbytes) {
 }
 
 // ---- forward launch ------------------------------------------------------------
-template <typename XT, typename YT, int VPL, int V>
+template <typename XT, typename YT, int VPL, int V, bool COMP = false>
 int launch_fwd_t(cbm_plan* P, const FwdArgs& a, cudaStream_t st) {
   static int grid_cache = 0, grid_dev = -1;
   if (grid_dev != P->device) {
-    grid_cache = grid_for(fwd_kernel<XT, YT, VPL, V>, P->device);
+    grid_cache = grid_for(fwd_kernel<XT, YT, VPL, V, COMP>, P->device);
     grid_dev = P->device;
   }
-  fwd_kernel<XT, YT, VPL, V><<<grid_cache, kThreads, 0, st>>>(a);
+  fwd_kernel<XT, YT, VPL, V, COMP><<<grid_cache, kThreads, 0, st>>>(a);
   P->launches++;
   P->last_grid = grid_cache;
   return cuda_status(cudaGetLastError());
@@ -146,8 +151,11 @@ bool staged_shape(int64_t nvec, int v, int forced, int* team, int* vpl) {
 template <typename XT, typename YT, int TL>
 int launch_staged_team(cbm_plan* P, const FwdArgs& a, int vpl, cudaStream_t st) {
   constexpr int V = 16 / (int)sizeof(XT);
+  // one piece per lane: a deeper ring (16 slots, 32 KiB per block) keeps as
+  // many bytes in flight as two pieces in 8 slots
+  constexpr int S1 = TL >= 16 ? 16 : 8;
   switch (vpl) {
-    case 1: return launch_stream_t<XT, YT, TL, 1, V, 8>(P, a, st);
+    case 1: return launch_stream_t<XT, YT, TL, 1, V, S1>(P, a, st);
     case 2: return launch_stream_t<XT, YT, TL, 2, V, 8>(P, a, st);
     case 4: return launch_stream_t<XT, YT, TL, 4, V, 8>(P, a, st);
     default:
@@ -169,14 +177,24 @@ int launch_staged(cbm_plan* P, const FwdArgs& a, int32_t xdt, int32_t ydt, int t
   return launch_staged_any<__nv_bfloat16, __nv_bfloat16>(P, a, team, vpl, st);
 }
 
-template <typename XT, typename YT, int V>
+template <typename XT, typename YT, int V, bool COMP = false>
 int launch_fwd_v(cbm_plan* P, const FwdArgs& a, int vpl, cudaStream_t st) {
   switch (vpl) {
-    case 1: return launch_fwd_t<XT, YT, 1, V>(P, a, st);
-    case 2: return launch_fwd_t<XT, YT, 2, V>(P, a, st);
-    case 4: return launch_fwd_t<XT, YT, 4, V>(P, a, st);
-    default: return launch_fwd_t<XT, YT, 8, V>(P, a, st);
+    case 1: return launch_fwd_t<XT, YT, 1, V, COMP>(P, a, st);
+    case 2: return launch_fwd_t<XT, YT, 2, V, COMP>(P, a, st);
+    case 4: return launch_fwd_t<XT, YT, 4, V, COMP>(P, a, st);
+    default: return launch_fwd_t<XT, YT, 8, V, COMP>(P, a, st);
   }
+}
+
+// compensated propagation: BF16 X only (the precision form), register kernel
+int launch_fwd_comp(cbm_plan* P, const FwdArgs& a, int32_t ydt, bool vec, int vpl, cudaStream_t st) {
+  if (ydt == CBM_F32) {
+    return vec ? launch_fwd_v<__nv_bfloat16, float, 8, true>(P, a, vpl, st)
+               : launch_fwd_v<__nv_bfloat16, float, 1, true>(P, a, vpl, st);
+  }
+  return vec ? launch_fwd_v<__nv_bfloat16, __nv_bfloat16, 8, true>(P, a, vpl, st)
+             : launch_fwd_v<__nv_bfloat16, __nv_bfloat16, 1, true>(P, a, vpl, st);
 }
 
 int launch_fwd(cbm_plan* P, const FwdArgs& a, int32_t xdt, int32_t ydt, bool vec, int vpl, cudaStream_t st) {
@@ -302,7 +320,8 @@ int rebuild_adjoint_chunks(cbm_plan* P, cudaStream_t st) {
 }
 
 // Reverse-propagation items (internal nodes, deepest first, with their
-// children) and the transposed delta matrix, both built once on the host.
+// children lists; built on the host) and the transposed delta matrix (sorted
+// on the device, transpose.cu), built once per plan.
 int build_adjoint(cbm_plan* P, cudaStream_t st) {
   if (P->adj_built) return CBM_OK;
   if (P->n_rows >= (int64_t)kInternalBit || P->n_cols >= (int64_t)kInternalBit) return CBM_ERR_INVALID;
@@ -350,25 +369,6 @@ int build_adjoint(cbm_plan* P, cudaStream_t st) {
   }
   P->n_rev_items = (int64_t)rnode.size();
   P->n_rev_chunks = n_rev_chunks;
-  // transposed delta: column j lists (row v or its slot, sign)
-  P->h_t_ptr.assign(P->n_cols + 1, 0);
-  for (int64_t k = 0; k < P->nnz; ++k) P->h_t_ptr[(P->h_ent[k] & 0x7fffffffu) + 1]++;
-  for (int64_t j = 0; j < P->n_cols; ++j) P->h_t_ptr[j + 1] += P->h_t_ptr[j];
-  std::vector<uint32_t> tent(P->nnz);
-  {
-    std::vector<int64_t> fill(P->h_t_ptr.begin(), P->h_t_ptr.end() - 1);
-    // visit rows in node order so each column's list is sorted by row
-    std::vector<int64_t> item_of(n);
-    for (int64_t i = 0; i < n; ++i) item_of[P->h_order[i]] = i;
-    for (int64_t v = 0; v < n; ++v) {
-      const int64_t i = item_of[v];
-      const uint32_t rv = P->h_slot[v] >= 0 ? ((uint32_t)P->h_slot[v] | kInternalBit) : (uint32_t)v;
-      for (int64_t k = P->h_ptr[i]; k < P->h_ptr[i + 1]; ++k) {
-        const uint32_t e = P->h_ent[k];
-        tent[fill[e & 0x7fffffffu]++] = rv | (e & 0x80000000u);
-      }
-    }
-  }
   int rc;
   if ((rc = upload(&P->d_rev_node, rnode, st, P->adj_bufs))) return rc;
   if ((rc = upload(&P->d_rev_chunk0, rchunk0, st, P->adj_bufs))) return rc;
@@ -378,8 +378,8 @@ int build_adjoint(cbm_plan* P, cudaStream_t st) {
   if ((rc = upload(&P->d_rev_ptr, rptr, st, P->adj_bufs))) return rc;
   if ((rc = upload(&P->d_rev_ent, rent, st, P->adj_bufs))) return rc;
   if ((rc = zeros_u32(&P->d_adj_flag, P->n_internal, st, P->adj_bufs))) return rc;
-  if ((rc = upload(&P->d_t_ptr, P->h_t_ptr, st, P->adj_bufs))) return rc;
-  if ((rc = upload(&P->d_t_ent, tent, st, P->adj_bufs))) return rc;
+  // transposed delta: column j lists (row v or its slot, sign), sorted on the GPU
+  if ((rc = transpose_on_device(P, st))) return rc;
   P->adj_built = true;
   return rebuild_adjoint_chunks(P, st);
 }
@@ -424,7 +424,8 @@ int64_t cbm_plan_workspace_bytes(const cbm_plan* P, int32_t op, int64_t n_cols, 
     const int64_t t_chunks = P->adj_built ? P->n_t_chunks : (2 * P->nnz / P->chunk_nnz + 1);
     rows = P->n_internal + t_chunks + (P->adj_built ? P->n_rev_chunks : P->n_internal);
   } else {
-    rows = P->n_chunks + (y_dtype == CBM_BF16 ? P->n_internal : 0);
+    rows = P->n_chunks + (y_dtype == CBM_BF16 ? P->n_internal : 0) +
+           (comp_active(P, x_dtype) ? P->n_internal : 0);
   }
   return align256(rows * ldp * 4) + 256;
 }
@@ -465,7 +466,8 @@ int cbm_matmul(cbm_plan* P, int32_t op, const void* x, int32_t xdt, int64_t ldx,
   if (needs_mult && (!P->d_mult || P->n_rows != P->n_cols)) return CBM_ERR_UNSUPPORTED;
   if ((op == CBM_OP_VALUES_ADD || op == CBM_OP_VALUES_RATIO) && xdt != CBM_F32) return CBM_ERR_DTYPE;
   const int64_t need = cbm_plan_workspace_bytes(P, op, n_cols, xdt, ydt, 0);
-  const bool need_ws = P->n_chunks > 0 || (ydt == CBM_BF16 && P->n_internal > 0);
+  const bool comp = comp_active(P, xdt);
+  const bool need_ws = P->n_chunks > 0 || (ydt == CBM_BF16 && P->n_internal > 0) || comp;
   if (need_ws && (!ws || ws_bytes < need)) return CBM_ERR_WORKSPACE;
   if (ws && reinterpret_cast<uintptr_t>(ws) % 16 != 0) return CBM_ERR_INVALID;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -519,6 +521,13 @@ int cbm_matmul(cbm_plan* P, int32_t op, const void* x, int32_t xdt, int64_t ldx,
     a.ldp = (int32_t)ldp;
     a.partial = static_cast<float*>(ws);
     a.pstate = ws ? static_cast<float*>(ws) + P->n_chunks * ldp : nullptr;
+    a.comp_item0 = (int32_t)P->n_items;
+    a.comp_read0 = (int32_t)P->n_items;
+    if (comp) {
+      a.pcomp = static_cast<float*>(ws) + (P->n_chunks + (ydt == CBM_BF16 ? P->n_internal : 0)) * ldp;
+      a.comp_item0 = (int32_t)P->level_start[P->comp_depth];
+      a.comp_read0 = (int32_t)P->level_start[std::min<int64_t>(P->comp_depth + 1, P->levels)];
+    }
     a.scale_mode = scale;
     a.prop_mode = prop;
     a.team = team;
@@ -536,7 +545,9 @@ int cbm_matmul(cbm_plan* P, int32_t op, const void* x, int32_t xdt, int64_t ldx,
     const bool staged = sh.vec && P->variant != CBM_VARIANT_REGISTER &&
                         staged_shape(nvec, sh.v, P->staged_team, &s_team, &s_vpl);
     int rc;
-    if (staged) {
+    if (comp) {
+      rc = launch_fwd_comp(P, a, ydt, sh.vec, vpl, st);
+    } else if (staged) {
       a.team = s_team;
       rc = launch_staged(P, a, xdt, ydt, s_team, s_vpl, st);
     } else {
@@ -560,18 +571,10 @@ int cbm_matmul_host(cbm_plan* P, int32_t op, const void* x_host, int32_t xdt, in
   int64_t w = slab_cols == 0 ? n_cols : std::min(slab_cols, n_cols);
   const int64_t unit = 16 / std::min(xs, ys);
   if (w < n_cols && w % unit != 0) w = std::min(n_cols, (w + unit - 1) / unit * unit);
-  // slab boundaries: the first and the last slab are half as wide (rounded to
-  // the 16-byte unit), since the copy-in of the first and the copy-out of the
-  // last overlap nothing; the others are w wide
+  // slab boundaries: w columns each, the last one the remainder (slabs narrower
+  // than 256 bytes make the strided copies slow, so they are not tapered)
   std::vector<int64_t> bounds(1, 0);
-  const int64_t h = std::max(unit, (w / 2 + unit - 1) / unit * unit);
-  if (w < n_cols && n_cols >= w + 2 * h) {
-    bounds.push_back(h);
-    while (n_cols - bounds.back() > w + h) bounds.push_back(bounds.back() + w);
-    if (n_cols - bounds.back() > h) bounds.push_back(n_cols - h);
-  } else {
-    while (n_cols - bounds.back() > w) bounds.push_back(bounds.back() + w);
-  }
+  while (n_cols - bounds.back() > w) bounds.push_back(bounds.back() + w);
   bounds.push_back(n_cols);
   const int64_t n_slabs = (int64_t)bounds.size() - 1;
   if (n_slabs > 4096) return CBM_ERR_INVALID;

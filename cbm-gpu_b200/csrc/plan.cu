@@ -284,6 +284,7 @@ int cbm_plan_create(const int32_t* row_ptr, const int32_t* col_idx, const float*
   std::vector<int64_t> lvl_start(max_depth + 2, 0);
   for (int64_t v = 0; v < n_rows; ++v) lvl_start[depth[v] + 1]++;
   for (int32_t l = 0; l <= max_depth; ++l) lvl_start[l + 1] += lvl_start[l];
+  P->level_start = lvl_start;
   std::vector<int32_t> order(n_rows);
   {
     std::vector<int64_t> fill(lvl_start.begin(), lvl_start.end() - 1);
@@ -401,6 +402,12 @@ int cbm_plan_tune(cbm_plan* P, int32_t chunk_nnz, int32_t rows_per_claim, int32_
     rc = rebuild_adjoint_chunks(P, st);
     if (rc) return rc;
   }
+  return CBM_OK;
+}
+
+int cbm_plan_set_compensation(cbm_plan* P, int32_t min_depth) {
+  if (!P || min_depth < -1) return CBM_ERR_INVALID;
+  P->comp_depth = min_depth;
   return CBM_OK;
 }
 

@@ -23,6 +23,10 @@ struct cbm_plan {
   int64_t launches = 0;
   int64_t last_grid = 0;
   long long timeout_ns = 1000000000ll;  // bounded waits: 1 s
+  // BF16 X: rows at tree depth >= comp_depth add their parent with compensated
+  // (TwoSum) arithmetic and carry the rounding residual (-1: never)
+  int32_t comp_depth = 64;
+  std::vector<int64_t> level_start;  // first item of each tree level, [levels + 1]
 
   // host copies used to rebuild chunk tables and the adjoint layout
   std::vector<int64_t> h_ptr;     // entry offsets per item (level order)
@@ -91,4 +95,5 @@ void free_all(std::vector<void*>& v);
 int build_layout(cbm_plan* P, cudaStream_t st);
 int rebuild_adjoint_chunks(cbm_plan* P, cudaStream_t st);
 void release_pipeline(cbm_plan* P);
+int transpose_on_device(cbm_plan* P, cudaStream_t st);
 }  // namespace cbm

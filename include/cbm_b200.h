@@ -174,7 +174,8 @@ int cbm_matmul(cbm_plan* plan, int32_t op, const void* x, int32_t x_dtype, int64
  * copies): X is copied in and Y out in column slabs of slab_cols columns (0:
  * one slab), with the host-to-device copy of slab k+1, the product of slab k
  * and the device-to-host copy of slab k-1 overlapped on two copy streams of
- * the plan and `stream`.  x_host [n_cols(A), n_cols] with leading dimension
+ * the plan and `stream` (64 fp32 columns, 256-byte row pieces, is the
+ * measured best on B200 over PCIe).  x_host [n_cols(A), n_cols] with leading dimension
  * ldx_host, y_host [n_rows(A), n_cols] with ldy_host; x_dev / y_dev: device
  * buffers of the same shapes, contiguous (the caller's: nothing is
  * allocated); workspace as for cbm_matmul with slab_cols columns.  Returns
@@ -197,12 +198,28 @@ int cbm_matmul_adjoint(cbm_plan* plan, int32_t op, const void* g, int32_t g_dtyp
  * delta matrix) ahead of the first cbm_matmul_adjoint; synchronous. */
 int cbm_plan_prepare_adjoint(cbm_plan* plan, void* stream);
 
+/* Precision form (BF16 X): rows at tree depth >= min_depth add their parent's
+ * row with compensated arithmetic (an error-free TwoSum per element, the
+ * rounding residual carried down the chain in an FP32 workspace row per
+ * internal node), so a chain's error stays that of one rounding instead of
+ * growing with its depth.  Applies when the tree has more than min_depth
+ * levels; such products run on the register-gather kernel.  -1: never;
+ * default 64 (below it an FP32 chain's rounding, depth * 2^-24 relative,
+ * stays under 4e-6).  FP32 X keeps the reference's plain rounding (parity). */
+int cbm_plan_set_compensation(cbm_plan* plan, int32_t min_depth);
+
 /* Limit of every device-side wait, in nanoseconds (default 1 s). */
 int cbm_plan_set_timeout(cbm_plan* plan, int64_t ns);
 
 /* Test hook: make queue item `item` wait on `parent_node` (whose ready flag may
  * never be set) to exercise the bounded wait.  -1 removes the parent. */
 int cbm_plan_debug_set_parent(cbm_plan* plan, int64_t item, int32_t parent_node, void* stream);
+
+/* Test hook: builds the adjoint layout if needed, rebuilds its transposed
+ * delta matrix on the host (a counting sort) and compares it word for word
+ * with the one sorted on the device: CBM_OK if equal, CBM_ERR_INTERNAL if not.
+ * Synchronous. */
+int cbm_plan_debug_check_transpose(cbm_plan* plan, void* stream);
 
 /* Synchronises `stream`, returns the first device-side error recorded since
  * the last call (CBM_OK, CBM_ERR_TIMEOUT, CBM_ERR_INDEX) in *device_status and

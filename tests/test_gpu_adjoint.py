@@ -175,3 +175,36 @@ def test_adjoint_many_children(cols):
     ref = _adj_f64("ax", ei, a.num_nodes, g)
     assert np.abs(dx.cpu().numpy() - ref).max() <= 1e-4 * np.abs(ref).max()
     a.plan.check_device()
+
+
+@pytest.mark.parametrize("graph", ["near_dup", "directed", "chain", "hub"])
+def test_transposed_index_sorted_on_device_equals_host_counting_sort(graph):
+    """The adjoint's transposed delta matrix is sorted on the GPU (radix sort of
+    (column, row) keys); a host counting sort must give the same words."""
+    from cbm import _lib
+
+    if graph == "near_dup":
+        ei, n = near_dup_graph(4000, seed=3), 4000
+    elif graph == "directed":
+        n = 3000
+        ei = random_graph(n, 6, seed=9, symmetric=False)
+    elif graph == "chain":
+        ei, n = chain_graph(500)
+    else:
+        # one column gathered by every row: a long transposed list (chunked)
+        n = 2000
+        r = np.arange(1, n, dtype=np.int32)
+        ei = np.concatenate([np.stack([r, np.zeros_like(r)]), np.stack([np.zeros_like(r), r])], axis=1)
+        ei = np.ascontiguousarray(ei[:, np.lexsort((ei[1], ei[0]))])
+    a = _make("ax", ei)
+    p = a.plan
+    assert p._lib.cbm_plan_debug_check_transpose(p._h, None) == _lib.OK
+    g = torch.randn(a.num_nodes, 40, device="cuda")
+    d1 = torch.empty_like(g)
+    d2 = torch.empty_like(g)
+    a.adjoint(g, d1)
+    a.adjoint(g, d2)
+    assert torch.equal(d1, d2)
+    ref = _adj_f64("ax", ei, a.num_nodes, g)
+    assert np.abs(d1.cpu().numpy() - ref).max() <= 1e-4 * max(1.0, np.abs(ref).max())
+    p.check_device()

@@ -53,3 +53,60 @@ def test_precision_form_error_vs_fp64():
     assert product["rel_fro"] <= 1e-5
     assert end_to_end["rel_fro"] <= 1e-2
     a.plan.check_device()
+
+
+def _threshold_graph(n):
+    """Symmetric A[i][j] = 1 iff i + j >= n - 1 (i != j): every row is its
+    predecessor plus about one column, so the CBM tree is one chain about n deep."""
+    i, j = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    r, c = np.nonzero((i + j >= n - 1) & (i != j))
+    return np.stack([r, c]).astype(np.int32)
+
+
+@pytest.mark.parametrize("op", ["ax", "adx", "dadx"])
+@pytest.mark.parametrize("ydt", [torch.float32, torch.bfloat16])
+def test_compensated_propagation_on_a_deep_chain(op, ydt):
+    """BF16 X on a 1,500-deep chain: with compensated propagation (the default
+    from depth 64 on) the error against FP64 of the same BF16 values stays at
+    about one FP32 rounding; with it switched off it grows with the depth."""
+    from cbm.cbm4ad import cbm4ad
+    from cbm.cbm4dad import cbm4dad
+    from cbm.cbm4mm import cbm4mm
+    from oracle import oracle
+
+    n = 1500
+    ei = _threshold_graph(n)
+    cls = {"ax": cbm4mm, "adx": cbm4ad, "dadx": cbm4dad}[op]
+    a = cls(torch.from_numpy(ei), torch.ones(ei.shape[1]), alpha=0)
+    assert a.plan.stats["levels"] > 1000
+    g = torch.Generator(device="cuda").manual_seed(5)
+    x = torch.randn(n, 64, device="cuda", generator=g).to(torch.bfloat16)
+    ptr, idx = oracle.csr_from_edges(ei, n)
+    dinv = 1.0 / np.sqrt(np.diff(ptr).astype(np.float64))
+    ref = oracle.dense_f64(ptr, idx, n, x.double().cpu().numpy(), rs=dinv if op == "dadx" else None,
+                           cs=dinv if op != "ax" else None)
+
+    def run():
+        y = torch.empty(n, 64, device="cuda", dtype=ydt)
+        a.matmul(x, y)
+        a.plan.check_device()
+        return float(np.abs(y.double().cpu().numpy() - ref).max() / np.abs(ref).max())
+
+    err_comp = run()
+    a.plan.set_compensation(-1)
+    err_plain = run()
+    a.plan.set_compensation(64)
+    print(f"{op} {ydt}: compensated {err_comp:.3g}, plain {err_plain:.3g}")
+    if ydt == torch.float32:
+        assert err_comp <= 2.5e-7
+        if op == "ax":
+            # +-1 sums of BF16 values are exact in FP32 at these magnitudes: there
+            # is no chain error to remove, and compensation must not add any
+            assert err_comp <= err_plain
+        else:
+            # scaled entries (ADX) and the ratio rule (DADX) round at every level
+            assert err_comp * 4 < err_plain
+    else:
+        # BF16 output: the final rounding (2^-9 relative) dominates both
+        assert err_comp <= 2.0 ** -8
+        assert err_comp <= err_plain * 1.01
