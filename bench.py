@@ -341,7 +341,13 @@ def run_precision(args):
     from cbm.cbm4ad import cbm4ad
 
     t0 = time.time()
-    ei, n, spec = synthetic.workload("powerlaw-2.4m")
+    if args.prec_nodes:
+        # the same law at another size (profiling runs)
+        n = args.prec_nodes
+        ei = synthetic._w_powerlaw(n, 2.3, 50.0, 0.40, 0.05, 2)
+        spec = {"alpha": 16}
+    else:
+        ei, n, spec = synthetic.workload("powerlaw-2.4m")
     a = cbm4ad(torch.from_numpy(ei), torch.ones(ei.shape[1]), alpha=spec["alpha"])
     a.plan.tune(chunk_nnz=args.chunk_nnz, rows_per_claim=args.rows_per_claim, variant=args.variant,
                 hot_rows=args.hot_rows, team=args.team)
@@ -359,7 +365,8 @@ def run_precision(args):
     line = {"metric": "CBM A.D^-1/2.X GB/s (algorithmic bytes), BF16 X", "value": b_alg / (ms * 1e-3) / 1e9,
             "unit": "GB/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "dtype": "bf16 X, f32 Y, f32 accumulate", "data": "synthetic",
-            "config": {"workload": "powerlaw-2.4m A D^-1/2 X", "nodes": n,
+            "config": {"workload": f"powerlaw (exponent 2.3, mean degree 50, 40% near-duplicates) N={n} A D^-1/2 X",
+                       "nodes": n,
                        "nnz_a": a.structure_stats["nnz_a"], "nnz_delta": st["nnz"], "tree_edges": st["edges"],
                        "cols": 128, "alpha": spec["alpha"], "setup_s": setup_s},
             "rows_per_s": n / (ms * 1e-3),
@@ -394,6 +401,7 @@ def main():
     ap.add_argument("--team", type=int, default=0)
     ap.add_argument("--hot-rows", type=int, default=65536)
     ap.add_argument("--slab-cols", type=int, default=64, help="column slab of the host-operand product (e2e)")
+    ap.add_argument("--prec-nodes", type=int, default=0, help="precision workload at this many nodes (same law)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
