@@ -19,7 +19,7 @@ NOALLOC_MAX_ROWS = 1048544
 F32, BF16 = 0, 1
 OP_AX, OP_ADX, OP_DADX, OP_VALUES_ADD, OP_VALUES_RATIO, OP_DAD_ADD = range(6)
 INPUT_DEVICE, INPUT_HOST = 0, 1
-VARIANT_AUTO, VARIANT_REGISTER, VARIANT_STAGED = 0, 1, 2
+VARIANT_AUTO, VARIANT_REGISTER, VARIANT_STAGED, VARIANT_TMA = 0, 1, 2, 3
 BUILD_EXHAUSTIVE = 1
 COALESCE_SYMMETRIZE, COALESCE_DROP_SELF = 1, 2
 S_DELTA_ROW, S_DELTA_COL, S_DELTA_VAL, S_BRANCHES, S_SRC, S_DST, S_PARENT, S_CSR_PTR, S_CSR_COL, \

@@ -103,7 +103,8 @@ class Plan:
         torch.cuda.current_stream(self.device).synchronize()
 
     def tune(self, chunk_nnz=256, rows_per_claim=4, variant="auto", hot_rows=65536, team=0, rows_per_claim_deep=0):
-        v = {"auto": _lib.VARIANT_AUTO, "register": _lib.VARIANT_REGISTER, "staged": _lib.VARIANT_STAGED}[variant]
+        v = {"auto": _lib.VARIANT_AUTO, "register": _lib.VARIANT_REGISTER, "staged": _lib.VARIANT_STAGED,
+             "tma": _lib.VARIANT_TMA}[variant]
         _lib.check(self._lib.cbm_plan_tune(self._h, int(chunk_nnz), int(rows_per_claim), int(rows_per_claim_deep), v,
                                            int(hot_rows), int(team), _stream(self.device)), "cbm_plan_tune")
         self._ws.clear()

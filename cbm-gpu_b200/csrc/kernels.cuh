@@ -18,6 +18,7 @@
 // size.  Every wait is still bounded (globaltimer), recording CBM_ERR_TIMEOUT.
 #pragma once
 
+#include <cuda.h>  // CUtensorMap (the TMA descriptor type)
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -97,6 +98,7 @@ struct FwdArgs {
   int32_t comp_item0;
   int32_t comp_read0;
   float* pcomp;        // [n_internal, ldp] residual rows of internal nodes
+  int32_t tma_rb;      // TMA variant: bytes of one gathered row (nvec * 16)
   long long timeout_ns;
 };
 
@@ -573,6 +575,56 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// ---- TMA (tile::gather4) and mbarrier helpers ------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+// makes initialised barriers visible to the TMA unit (the async proxy)
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// orders this thread's earlier generic-proxy shared-memory accesses before
+// later async-proxy (TMA) writes
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// four rows r0..r3 of a 2-D tensor (box: all columns from col0, one row high)
+// into dst, one after another; completion counted on bar
+__device__ __forceinline__ void tma_gather4(void* dst, const CUtensorMap* map, int col0, int r0, int r1, int r2, int r3,
+                                            uint64_t* bar, uint64_t policy) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes.L2::cache_hint"
+      " [%0], [%1, {%2, %3, %4, %5, %6}], [%7], %8;" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(col0), "r"(r0), "r"(r1), "r"(r2), "r"(r3), "r"(smem_u32(bar)),
+      "l"(policy)
+      : "memory");
+}
+// Bounded wait for a barrier phase: try_wait (which itself suspends for a
+// while) until the phase completes or timeout_ns pass.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, long long timeout_ns) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (long long it = 0; it < kMaxSpins; ++it) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((long long)(global_ns() - t0) > timeout_ns) break;
+  }
+  return false;
+}
+
 template <typename XT, int V>
 __device__ __forceinline__ void unpack16(const uint4& r, float (&o)[V]) {
   if constexpr (sizeof(XT) == 4) {
@@ -770,9 +822,172 @@ __device__ __forceinline__ void stream_pass(const XT* __restrict__ x, int64_t ld
   if (ls) __syncwarp();
 }
 
-template <typename XT, typename YT, int TL, int VPL, int V, int S, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) fwd_stream_kernel(const FwdArgs a) {
-  extern __shared__ uint4 ring[];
+// TMA variant of stream_pass: the team's rows come in groups of four by one
+// tile::gather4 copy (issued by the team's first lane) into the team's ring of
+// G slots of four rows, completion counted on one mbarrier per slot.
+// Every lane owns every piece of a row here (nvec == TL * VPL, rows of 16-byte
+// multiples, 128-byte multiples per row), so a lane reads pieces tl + v * TL of
+// each gathered row.  The summation order is stream_pass's (sequential FMAs
+// per row).  A wait that runs out records CBM_ERR_TIMEOUT and stops further
+// copies; the copies already issued are waited for (bounded) before return.
+template <typename XT, int TL, int VPL, int V, int G, typename NextEnd, typename OnEnd>
+__device__ __forceinline__ void stream_pass_tma(const CUtensorMap* tmap, int rb, const uint32_t* __restrict__ ent,
+                                                const float* __restrict__ val, int64_t k0, int len, int scale_mode,
+                                                const float* __restrict__ mult, uint8_t* tring, uint64_t* tbar,
+                                                unsigned& phase, int tl, unsigned tmask, NextEnd next_end,
+                                                OnEnd on_end, const float& row_dv, bool hints, bool lockstep,
+                                                QueueState* qs, long long timeout_ns) {
+  static_assert(G >= 2 && (G & (G - 1)) == 0 && 4 * G <= TL, "G slots of four rows, 4G entries within two batches");
+  uint64_t pol_keep, pol_stream;
+  if (hints) {
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol_keep));
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol_stream));
+  } else {
+    asm volatile("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(pol_keep));
+    pol_stream = pol_keep;
+  }
+  const uint32_t* ent0 = ent + k0;
+  const float* val0 = val ? val + k0 : nullptr;
+  // a failure earlier in this launch: no more copies (the results are void)
+  bool broken = *(volatile int*)&qs->error != 0;
+
+  int bA = 0;
+  uint32_t eA = 0, eB = 0, eC = 0;
+  float sA = 0.f, sB = 0.f;
+  {
+    const int ia = tl, ib = TL + tl, ic = 2 * TL + tl;
+    if (ia < len) eA = __ldcs(ent0 + ia);
+    if (ib < len) eB = __ldcs(ent0 + ib);
+    if (ic < len) eC = __ldcs(ent0 + ic);
+    sA = entry_scale(eA, ia, ia < len, scale_mode, mult, val0);
+    sB = entry_scale(eB, ib, ib < len, scale_mode, mult, val0);
+  }
+  int issued = 0;  // groups issued so far (group g: entries 4g .. 4g + 3)
+  // entries of group g lie in batches A and B: the consumer is at 4g - 4G or
+  // later, and 4G <= TL
+  auto issue = [&](int g) {
+    const int p0 = 4 * g;
+    if (p0 >= len || broken) return;
+    uint32_t e4[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int p = p0 + u < len ? p0 + u : len - 1;  // padding repeats the last row
+      e4[u] = __shfl_sync(tmask, p < bA + TL ? eA : eB, p & (TL - 1), TL);
+    }
+    if (tl == 0) {
+      const int sl = g & (G - 1);
+      const uint64_t pol = ((e4[0] | e4[1] | e4[2] | e4[3]) & kHotBit) ? pol_keep : pol_stream;
+      fence_proxy_async();
+      mbar_expect_tx(tbar + sl, 4u * (unsigned)rb);
+      tma_gather4(tring + (size_t)sl * 4 * rb, tmap, 0, (int)(e4[0] & kColMask), (int)(e4[1] & kColMask),
+                  (int)(e4[2] & kColMask), (int)(e4[3] & kColMask), tbar + sl, pol);
+    }
+    issued = g + 1;
+  };
+#pragma unroll
+  for (int g = 0; g < G; ++g) issue(g);
+
+  float acc[VPL][V];
+#pragma unroll
+  for (int v = 0; v < VPL; ++v)
+#pragma unroll
+    for (int q = 0; q < V; ++q) acc[v][q] = 0.f;
+  int end_at = next_end();
+  const bool ls = TL < 32 && lockstep;
+  const int wlen = ls ? __reduce_max_sync(0xffffffffu, len) : len;
+  int waited = 0;  // groups waited for
+  auto consume = [&](int kk, const uint8_t* rowp, bool active) {
+    const float sc = __fmul_rn(__shfl_sync(tmask, sA, kk & (TL - 1), TL), row_dv);
+    if (active) {
+      const uint4* pr = reinterpret_cast<const uint4*>(rowp) + tl;
+#pragma unroll
+      for (int v = 0; v < VPL; ++v) {
+        float t[V];
+        unpack16<XT, V>(pr[v * TL], t);
+#pragma unroll
+        for (int q = 0; q < V; ++q) acc[v][q] = fmaf(sc, t[q], acc[v][q]);
+      }
+    }
+  };
+  for (int k = 0; k < wlen; k += 4) {
+    if (k == bA + TL) {
+      bA += TL;
+      eA = eB;
+      sA = sB;
+      eB = eC;
+      const int ib = bA + TL + tl, ic = bA + 2 * TL + tl;
+      sB = entry_scale(eB, ib, ib < len, scale_mode, mult, val0);
+      eC = ic < len ? __ldcs(ent0 + ic) : 0u;
+    }
+    const int g = k >> 2;
+    const int sl = g & (G - 1);
+    if (k < len && g < issued) {
+      if (mbar_wait_bounded(tbar + sl, (phase >> sl) & 1u, timeout_ns)) {
+        phase ^= 1u << sl;
+      } else if (!broken) {
+        broken = true;
+        if (tl == 0 && atomicCAS(&qs->error, 0, 8 /* CBM_ERR_TIMEOUT */) == 0) qs->error_info = -1 - (long long)g;
+      }
+      waited = g + 1;
+    }
+    const uint8_t* slot = tring + (size_t)sl * 4 * rb;
+    if (k + 4 <= len && end_at >= k + 4) {
+      float sc[4];
+      uint4 raw[4][VPL];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) sc[u] = __fmul_rn(__shfl_sync(tmask, sA, (k + u) & (TL - 1), TL), row_dv);
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < VPL; ++v) raw[u][v] = reinterpret_cast<const uint4*>(slot + u * rb)[tl + v * TL];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < VPL; ++v) {
+          float t[V];
+          unpack16<XT, V>(raw[u][v], t);
+#pragma unroll
+          for (int q = 0; q < V; ++q) acc[v][q] = fmaf(sc[u], t[q], acc[v][q]);
+        }
+    } else {
+      for (int u = 0; u < 4; ++u) {
+        const int kk = k + u;
+        const bool active = kk < len;
+        if (active) {
+          while (kk == end_at) {
+            on_end(acc);
+            end_at = next_end();
+          }
+        }
+        consume(kk, slot + u * rb, active);
+      }
+    }
+    // every lane of the team is done with the slot before it is refilled
+    __syncwarp(tmask);
+    issue(g + G);
+    if (ls) __syncwarp();
+  }
+  // after a failure: wait (bounded) for the copies still in flight
+  for (int g = waited; g < issued; ++g) {
+    const int sl = g & (G - 1);
+    if (mbar_wait_bounded(tbar + sl, (phase >> sl) & 1u, timeout_ns)) phase ^= 1u << sl;
+  }
+  while (end_at <= len) {
+    on_end(acc);
+    end_at = next_end();
+  }
+  if (ls) __syncwarp();
+}
+
+// TMA = true: rows arrive by tile::gather4 copies into per-team rings (the
+// dynamic shared memory then holds BLOCK / TL teams x S / 4 slots of four
+// rows of tma_rb bytes, followed by one mbarrier per slot: S entries in flight
+// per team, as in the cp.async ring); `tmap` describes
+// X (columns [0, nvec * V), every row, one-row box).  TMA = false: the
+// per-thread cp.async ring of stream_pass (tmap unused).
+template <typename XT, typename YT, int TL, int VPL, int V, int S, int BLOCK, bool TMA = false>
+__global__ void __launch_bounds__(BLOCK) fwd_stream_kernel(const FwdArgs a, const __grid_constant__ CUtensorMap tmap) {
+  extern __shared__ __align__(1024) uint4 ring[];
   const int lane = threadIdx.x & 31;
   const int team = lane / TL;
   const int tl = lane & (TL - 1);
@@ -782,6 +997,24 @@ __global__ void __launch_bounds__(BLOCK) fwd_stream_kernel(const FwdArgs a) {
   const XT* x = static_cast<const XT*>(a.x);
   const bool hints = a.hints != 0;
   float ch_dv = 1.f;
+  // TMA rings and barriers of this thread's team
+  uint8_t* tring = nullptr;
+  uint64_t* tbar = nullptr;
+  unsigned tphase = 0;
+  constexpr int G = S / 4;
+  if constexpr (TMA) {
+    constexpr int n_teams = BLOCK / TL;
+    const int bt = threadIdx.x / TL;
+    uint8_t* base = reinterpret_cast<uint8_t*>(ring);
+    tring = base + (size_t)bt * G * 4 * a.tma_rb;
+    tbar = reinterpret_cast<uint64_t*>(base + (size_t)n_teams * G * 4 * a.tma_rb) + bt * G;
+    if (tl == 0) {
+#pragma unroll
+      for (int g = 0; g < G; ++g) mbar_init(tbar + g, 1);
+      mbar_init_fence();
+    }
+    __syncwarp(tmask);
+  }
 
   // ---- chunks of long rows: one chunk per team per claim ----
   if (a.n_chunks > 0) {
@@ -816,8 +1049,13 @@ __global__ void __launch_bounds__(BLOCK) fwd_stream_kernel(const FwdArgs a) {
         done = true;
       };
       // chunks depend on nothing: always in lockstep
-      stream_pass<XT, TL, VPL, V, S, BLOCK>(x, a.ldx, a.nvec, a.cent, a.cval, cb, clen, a.scale_mode, a.mult,
-                                            ring, tl, tmask, next_end, on_end, ch_dv, hints, true);
+      if constexpr (TMA) {
+        stream_pass_tma<XT, TL, VPL, V, G>(&tmap, a.tma_rb, a.cent, a.cval, cb, clen, a.scale_mode, a.mult, tring, tbar,
+                                        tphase, tl, tmask, next_end, on_end, ch_dv, hints, true, a.qs, a.timeout_ns);
+      } else {
+        stream_pass<XT, TL, VPL, V, S, BLOCK>(x, a.ldx, a.nvec, a.cent, a.cval, cb, clen, a.scale_mode, a.mult,
+                                              ring, tl, tmask, next_end, on_end, ch_dv, hints, true);
+      }
     }
   }
 
@@ -987,8 +1225,14 @@ __global__ void __launch_bounds__(BLOCK) fwd_stream_kernel(const FwdArgs a) {
       };
       // a parent row inside this warp's claim: let the teams run independently
       const bool lockstep = !__any_sync(0xffffffffu, dep_in_claim);
-      stream_pass<XT, TL, VPL, V, S, BLOCK>(x, a.ldx, a.nvec, a.ent, a.val, k0, len, a.scale_mode, a.mult, ring,
-                                            tl, tmask, next_end, on_end, row_dv, hints, lockstep);
+      if constexpr (TMA) {
+        stream_pass_tma<XT, TL, VPL, V, G>(&tmap, a.tma_rb, a.ent, a.val, k0, len, a.scale_mode, a.mult, tring, tbar,
+                                        tphase, tl, tmask, next_end, on_end, row_dv, hints, lockstep, a.qs,
+                                        a.timeout_ns);
+      } else {
+        stream_pass<XT, TL, VPL, V, S, BLOCK>(x, a.ldx, a.nvec, a.ent, a.val, k0, len, a.scale_mode, a.mult, ring,
+                                              tl, tmask, next_end, on_end, row_dv, hints, lockstep);
+      }
     }
   }
   finish_block(a.qs, epoch);

@@ -106,12 +106,13 @@ int launch_fwd_t(cbm_plan* P, const FwdArgs& a, cudaStream_t st) {
 // 128 threads.
 constexpr int kStagedBlock = 128;
 
-template <typename XT, typename YT, int TL, int VPL, int V, int S>
-int launch_stream_t(cbm_plan* P, const FwdArgs& a, cudaStream_t st) {
-  static int grid_cache = 0, grid_dev = -1;
-  constexpr int smem = S * VPL * kStagedBlock * 16;
-  auto kern = fwd_stream_kernel<XT, YT, TL, VPL, V, S, kStagedBlock>;
-  if (grid_dev != P->device) {
+template <typename XT, typename YT, int TL, int VPL, int V, int S, bool TMA = false>
+int launch_stream_t(cbm_plan* P, const FwdArgs& a, const CUtensorMap& map, cudaStream_t st) {
+  static int grid_cache = 0, grid_dev = -1, grid_smem = -1;
+  constexpr int n_teams = kStagedBlock / TL;
+  const int smem = TMA ? n_teams * (S / 4) * (4 * a.tma_rb + 8) : S * VPL * kStagedBlock * 16;
+  auto kern = fwd_stream_kernel<XT, YT, TL, VPL, V, S, kStagedBlock, TMA>;
+  if (grid_dev != P->device || grid_smem != smem) {
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
       return CBM_ERR_CUDA;
     int per_sm = 0;
@@ -120,11 +121,51 @@ int launch_stream_t(cbm_plan* P, const FwdArgs& a, cudaStream_t st) {
       per_sm = 1;
     grid_cache = per_sm * sm_count(P->device);
     grid_dev = P->device;
+    grid_smem = smem;
   }
-  kern<<<grid_cache, kStagedBlock, smem, st>>>(a);
+  kern<<<grid_cache, kStagedBlock, smem, st>>>(a, map);
   P->launches++;
   P->last_grid = grid_cache;
   return cuda_status(cudaGetLastError());
+}
+
+// cuTensorMapEncodeTiled from the driver, found once through the runtime
+// (no link-time dependency on libcuda).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(f);
+  }
+  return fn;
+}
+
+// Tensor map of X for the gather: columns [0, cols) of `rows` rows with a
+// leading dimension of ldx elements; box = the whole width, one row high
+// (what tile::gather4 takes).  x 16-byte aligned, ldx * size a multiple of 16,
+// cols * size a multiple of 16 and cols <= 256 (checked by the caller).
+int encode_x_map(CUtensorMap* map, const void* x, int32_t xdt, int64_t rows, int64_t ldx, int64_t cols) {
+  EncodeTiledFn fn = encode_tiled();
+  if (!fn) return CBM_ERR_CUDA;
+  const int es = xdt == CBM_BF16 ? 2 : 4;
+  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)(ldx * es)};
+  const cuuint32_t box[2] = {(cuuint32_t)cols, 1u};
+  const cuuint32_t estr[2] = {1u, 1u};
+  const CUresult r = fn(map, xdt == CBM_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                        const_cast<void*>(x), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_NONE,
+                        cols * es >= 256 ? CU_TENSOR_MAP_L2_PROMOTION_L2_256B : CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? CBM_OK : CBM_ERR_CUDA;
 }
 
 // Team shape of the staged kernel for nvec 16-byte pieces per row.  A lane
@@ -149,32 +190,60 @@ bool staged_shape(int64_t nvec, int v, int forced, int* team, int* vpl) {
 }
 
 template <typename XT, typename YT, int TL>
-int launch_staged_team(cbm_plan* P, const FwdArgs& a, int vpl, cudaStream_t st) {
+int launch_staged_team(cbm_plan* P, const FwdArgs& a, int vpl, const CUtensorMap& map, cudaStream_t st) {
   constexpr int V = 16 / (int)sizeof(XT);
   // one piece per lane: a deeper ring (16 slots, 32 KiB per block) keeps as
   // many bytes in flight as two pieces in 8 slots
   constexpr int S1 = TL >= 16 ? 16 : 8;
   switch (vpl) {
-    case 1: return launch_stream_t<XT, YT, TL, 1, V, S1>(P, a, st);
-    case 2: return launch_stream_t<XT, YT, TL, 2, V, 8>(P, a, st);
-    case 4: return launch_stream_t<XT, YT, TL, 4, V, 8>(P, a, st);
+    case 1: return launch_stream_t<XT, YT, TL, 1, V, S1>(P, a, map, st);
+    case 2: return launch_stream_t<XT, YT, TL, 2, V, 8>(P, a, map, st);
+    case 4: return launch_stream_t<XT, YT, TL, 4, V, 8>(P, a, map, st);
     default:
-      if constexpr (V == 4) return launch_stream_t<XT, YT, TL, 8, V, 4>(P, a, st);
+      if constexpr (V == 4) return launch_stream_t<XT, YT, TL, 8, V, 4>(P, a, map, st);
       return CBM_ERR_INTERNAL;
   }
 }
 
 template <typename XT, typename YT>
-int launch_staged_any(cbm_plan* P, const FwdArgs& a, int team, int vpl, cudaStream_t st) {
-  if (team == 8) return launch_staged_team<XT, YT, 8>(P, a, vpl, st);
-  if (team == 16) return launch_staged_team<XT, YT, 16>(P, a, vpl, st);
-  return launch_staged_team<XT, YT, 32>(P, a, vpl, st);
+int launch_staged_any(cbm_plan* P, const FwdArgs& a, int team, int vpl, const CUtensorMap& map, cudaStream_t st) {
+  if (team == 8) return launch_staged_team<XT, YT, 8>(P, a, vpl, map, st);
+  if (team == 16) return launch_staged_team<XT, YT, 16>(P, a, vpl, map, st);
+  return launch_staged_team<XT, YT, 32>(P, a, vpl, map, st);
 }
 
 int launch_staged(cbm_plan* P, const FwdArgs& a, int32_t xdt, int32_t ydt, int team, int vpl, cudaStream_t st) {
-  if (xdt == CBM_F32) return launch_staged_any<float, float>(P, a, team, vpl, st);
-  if (ydt == CBM_F32) return launch_staged_any<__nv_bfloat16, float>(P, a, team, vpl, st);
-  return launch_staged_any<__nv_bfloat16, __nv_bfloat16>(P, a, team, vpl, st);
+  CUtensorMap none;
+  std::memset(&none, 0, sizeof(none));
+  if (xdt == CBM_F32) return launch_staged_any<float, float>(P, a, team, vpl, none, st);
+  if (ydt == CBM_F32) return launch_staged_any<__nv_bfloat16, float>(P, a, team, vpl, none, st);
+  return launch_staged_any<__nv_bfloat16, __nv_bfloat16>(P, a, team, vpl, none, st);
+}
+
+// TMA variant: every lane owns every piece (nvec == team * vpl), one or two
+// pieces per lane; ring depths as in the cp.async variant.
+template <typename XT, typename YT>
+int launch_tma_any(cbm_plan* P, const FwdArgs& a, int team, int vpl, const CUtensorMap& map, cudaStream_t st) {
+  constexpr int V = 16 / (int)sizeof(XT);
+  if (team == 8 && vpl == 1) return launch_stream_t<XT, YT, 8, 1, V, 8, true>(P, a, map, st);
+  if (team == 16 && vpl == 1) return launch_stream_t<XT, YT, 16, 1, V, 16, true>(P, a, map, st);
+  if (team == 32 && vpl == 1) return launch_stream_t<XT, YT, 32, 1, V, 16, true>(P, a, map, st);
+  if (team == 32 && vpl == 2) return launch_stream_t<XT, YT, 32, 2, V, 8, true>(P, a, map, st);
+  return CBM_ERR_INTERNAL;
+}
+
+int launch_tma(cbm_plan* P, const FwdArgs& a, int32_t xdt, int32_t ydt, int team, int vpl, const CUtensorMap& map,
+               cudaStream_t st) {
+  if (xdt == CBM_F32) return launch_tma_any<float, float>(P, a, team, vpl, map, st);
+  if (ydt == CBM_F32) return launch_tma_any<__nv_bfloat16, float>(P, a, team, vpl, map, st);
+  return launch_tma_any<__nv_bfloat16, __nv_bfloat16>(P, a, team, vpl, map, st);
+}
+
+// The TMA variant applies to 16-byte-vector rows of a power-of-two number of
+// pieces (8 .. 32 per team, at most 256 elements: one TMA box), one or two
+// pieces per lane.
+bool tma_shape(int64_t nvec, int v, int team, int vpl) {
+  return nvec >= 8 && (nvec & (nvec - 1)) == 0 && nvec == (int64_t)team * vpl && nvec * v <= 256 && vpl <= 2;
 }
 
 template <typename XT, typename YT, int V, bool COMP = false>
@@ -544,9 +613,16 @@ int cbm_matmul(cbm_plan* P, int32_t op, const void* x, int32_t xdt, int64_t ldx,
     int s_team = 0, s_vpl = 0;
     const bool staged = sh.vec && P->variant != CBM_VARIANT_REGISTER &&
                         staged_shape(nvec, sh.v, P->staged_team, &s_team, &s_vpl);
+    const bool tma = staged && P->variant == CBM_VARIANT_TMA && tma_shape(nvec, sh.v, s_team, s_vpl);
     int rc;
     if (comp) {
       rc = launch_fwd_comp(P, a, ydt, sh.vec, vpl, st);
+    } else if (tma) {
+      CUtensorMap map;
+      if ((rc = encode_x_map(&map, a.x, xdt, P->n_cols, ldx, cols))) return rc;
+      a.team = s_team;
+      a.tma_rb = (int32_t)(nvec * 16);
+      rc = launch_tma(P, a, xdt, ydt, s_team, s_vpl, map, st);
     } else if (staged) {
       a.team = s_team;
       rc = launch_staged(P, a, xdt, ydt, s_team, s_vpl, st);

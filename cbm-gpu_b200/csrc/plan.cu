@@ -389,7 +389,7 @@ int cbm_plan_tune(cbm_plan* P, int32_t chunk_nnz, int32_t rows_per_claim, int32_
   P->rows_per_claim_deep = rows_per_claim_deep;
   if (team != 0 && team != 8 && team != 16 && team != 32) return CBM_ERR_INVALID;
   P->staged_team = team;
-  if (variant < CBM_VARIANT_AUTO || variant > CBM_VARIANT_STAGED) return CBM_ERR_INVALID;
+  if (variant < CBM_VARIANT_AUTO || variant > CBM_VARIANT_TMA) return CBM_ERR_INVALID;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (cudaStreamSynchronize(st) != cudaSuccess) return CBM_ERR_CUDA;
   P->rows_per_claim = rows_per_claim;

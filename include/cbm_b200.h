@@ -151,7 +151,10 @@ int cbm_plan_set_multipliers(cbm_plan* plan, const float* d_multipliers, void* s
 enum {
   CBM_VARIANT_AUTO = 0,     /* staged where it applies, else register gather */
   CBM_VARIANT_REGISTER = 1, /* X rows gathered into registers, U entries at a time */
-  CBM_VARIANT_STAGED = 2    /* X rows staged through shared memory by cp.async */
+  CBM_VARIANT_STAGED = 2,   /* X rows staged through shared memory by cp.async */
+  CBM_VARIANT_TMA = 3       /* X rows gathered four at a time by TMA (tile::gather4) into
+                               per-team rings; rows of 8, 16 or 32 pieces of 16 bytes, at
+                               most 256 elements (else as STAGED) */
 };
 int cbm_plan_tune(cbm_plan* plan, int32_t chunk_nnz, int32_t rows_per_claim, int32_t rows_per_claim_deep,
                   int32_t variant, int64_t hot_rows, int32_t team, void* stream);
