@@ -37,6 +37,7 @@ REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(REPO, "cbm-gpu_b200"))
 
 WORKLOAD = "powerlaw-1m"
+CACHE = os.path.join(REPO, "_cache")  # generated graphs and constructed CBM structures
 COLS = 256
 HBM_FALLBACK_GBS = 6650.0
 
@@ -205,7 +206,7 @@ def run_reference(args, rank, world):
     from oracle import oracle
 
     ei, n, spec = load_graph(0, 1)
-    s = cbm_mkl_cpp.build(ei[0], ei[1], n, spec["alpha"])
+    s = cbm_mkl_cpp.build_cached(ei[0], ei[1], n, spec["alpha"], CACHE)
     crow, col = s.csr_ptr, s.csr_col
     deg = np.diff(oracle.csr_from_edges(ei, n)[0]).astype(np.float32)
     with np.errstate(divide="ignore"):
@@ -244,7 +245,7 @@ def gcn_timing(steps, warmup):
     from cbm.gcn import GCN, cross_entropy
 
     ei, n, spec = synthetic.workload("powerlaw-170k")
-    a = cbm4dad(torch.from_numpy(ei), torch.ones(ei.shape[1]), alpha=spec["alpha"])
+    a = cbm4dad(torch.from_numpy(ei), torch.ones(ei.shape[1]), alpha=spec["alpha"], cache_dir=CACHE)
     g = torch.Generator(device="cuda").manual_seed(3)
     x = torch.randn(n, 128, device="cuda", generator=g)
     labels = torch.randint(0, 40, (n,), device="cuda", generator=g)
@@ -348,7 +349,7 @@ def run_precision(args):
         spec = {"alpha": 16}
     else:
         ei, n, spec = synthetic.workload("powerlaw-2.4m")
-    a = cbm4ad(torch.from_numpy(ei), torch.ones(ei.shape[1]), alpha=spec["alpha"])
+    a = cbm4ad(torch.from_numpy(ei), torch.ones(ei.shape[1]), alpha=spec["alpha"], cache_dir=CACHE)
     a.plan.tune(chunk_nnz=args.chunk_nnz, rows_per_claim=args.rows_per_claim, variant=args.variant,
                 hot_rows=args.hot_rows, team=args.team)
     setup_s = time.time() - t0
@@ -440,7 +441,7 @@ def main():
     # weak scaling: rank r owns columns [c0, c1) of a [N, COLS * world] X and Y
     c0, c1 = column_shard(COLS * world, rank, world)
     assert c1 - c0 == COLS
-    a = cbm4dad(torch.from_numpy(ei), torch.ones(ei.shape[1]), alpha=spec["alpha"])
+    a = cbm4dad(torch.from_numpy(ei), torch.ones(ei.shape[1]), alpha=spec["alpha"], cache_dir=CACHE)
     a.plan.tune(chunk_nnz=args.chunk_nnz, rows_per_claim=args.rows_per_claim, variant=args.variant,
                 hot_rows=args.hot_rows, team=args.team)
     st = a.plan.stats

@@ -17,7 +17,7 @@ OK, ERR_INVALID, ERR_INDEX, ERR_ALLOC, ERR_CUDA, ERR_STRUCTURE, ERR_DTYPE, ERR_S
     ERR_UNSUPPORTED, ERR_WORKSPACE, ERR_INTERNAL, ERR_TOO_LARGE = range(13)
 NOALLOC_MAX_ROWS = 1048544
 F32, BF16 = 0, 1
-OP_AX, OP_ADX, OP_DADX, OP_VALUES_ADD, OP_VALUES_RATIO, OP_DAD_ADD = range(6)
+OP_AX, OP_ADX, OP_DADX, OP_VALUES_ADD, OP_VALUES_RATIO, OP_DAD_ADD, OP_GIN = range(7)
 INPUT_DEVICE, INPUT_HOST = 0, 1
 VARIANT_AUTO, VARIANT_REGISTER, VARIANT_STAGED, VARIANT_TMA = 0, 1, 2, 3
 BUILD_EXHAUSTIVE = 1
@@ -48,6 +48,7 @@ SIGNATURES = [
     ("cbm_matmul", C.c_int, [vp, i32, vp, i32, i64, vp, i32, i64, i64, vp, i64, vp]),
     ("cbm_matmul_adjoint", C.c_int, [vp, i32, vp, i32, i64, vp, i32, i64, i64, vp, i64, vp]),
     ("cbm_matmul_host", C.c_int, [vp, i32, vp, i32, i64, vp, i32, i64, i64, i64, vp, vp, vp, i64, vp]),
+    ("cbm_matmul_gin", C.c_int, [vp, C.c_float, vp, i32, i64, vp, i32, i64, i64, vp, i64, vp]),
     ("cbm_plan_prepare_adjoint", C.c_int, [vp, vp]),
     ("cbm_plan_set_timeout", C.c_int, [vp, i64]),
     ("cbm_plan_set_compensation", C.c_int, [vp, i32]),

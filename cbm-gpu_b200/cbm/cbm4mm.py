@@ -23,13 +23,15 @@ __all__ = ["cbm4mm"]
 class cbm4mm:  # noqa: N801 (the reference's class name)
     _op = "ax"
 
-    def __init__(self, edge_index, edge_values, alpha=0):
+    def __init__(self, edge_index, edge_values, alpha=0, cache_dir=None):
+        """cache_dir (an addition): reuse the constructed structure from an
+        on-disk cache keyed by the edge list and alpha (cbm_mkl_cpp.build_cached)."""
         if edge_index.numel() == 0:
             raise RuntimeError("edge_index is empty")
         num_rows = int(max(edge_index[0].max(), edge_index[1].max())) + 1
         if isinstance(edge_values, torch.Tensor) and edge_values.dtype != torch.float32:
             raise RuntimeError('"src_values" is not a tensor of type "torch::kFloat32"')
-        s = cbm_mkl.build(edge_index[0], edge_index[1], num_rows, alpha)
+        s = cbm_mkl.build_cached(edge_index[0], edge_index[1], num_rows, alpha, cache_dir)
         self.structure_stats = {"nnz_a": s.nnz_a, "nnz_delta": int(s.csr_col.size), "edges": int(s.src.size),
                                 "branches": int(s.branches.size) - 1, "candidates": s.n_candidates}
         self.deltas = torch.sparse_csr_tensor(
@@ -50,6 +52,12 @@ class cbm4mm:  # noqa: N801 (the reference's class name)
 
     def matmul(self, x, y):
         self._plan.matmul(self._op, x, y)
+
+    def matmul_add(self, x, y, epsilon=0.0):
+        """y <- A x + (1 + epsilon) x: the GIN aggregation the reference computes
+        on the CPU only (s_spmm_update_add_csr_int32,
+        cbm/cbm_extensions.cpp:498-591), with the binary A of this matrix."""
+        self._plan.matmul_gin(x, y, epsilon)
 
     def matmul_host(self, x, y, slab_cols=64):
         """y <- (this operator) x for host tensors x and y (pinned for full-speed

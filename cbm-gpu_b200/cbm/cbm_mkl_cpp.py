@@ -23,7 +23,10 @@ import torch
 
 from . import _lib
 
-__all__ = ["init", "build", "Structure"]
+__all__ = ["init", "build", "build_cached", "save_structure", "load_structure", "Structure"]
+
+# on-disk format: an .npz of every Structure array plus these scalars
+_FORMAT = "cbm-structure-1"
 
 
 @dataclass
@@ -112,3 +115,60 @@ def init(src_row_idx, src_col_idx, src_values, src_n_rows, alpha):
     s = build(src_row_idx, src_col_idx, int(src_n_rows), int(alpha))
     return [torch.from_numpy(getattr(s, f)) for f in
             ("delta_row", "delta_col", "delta_val", "branches", "src", "dst")]
+
+
+def save_structure(path, s, key=""):
+    """Writes a Structure as an uncompressed .npz (atomically: a temporary file,
+    then a rename).  ``key`` records what it was built from."""
+    import os
+
+    arrays = {name: getattr(s, name) for name, _, _ in _FIELDS}
+    meta = np.array([s.n, s.n_candidates, s.tree_cost, s.nnz_a], dtype=np.int64)
+    tmp = f"{path}.tmp{os.getpid()}"
+    with open(tmp, "wb") as f:
+        np.savez(f, _format=np.array(_FORMAT), _key=np.array(key), _meta=meta, **arrays)
+    os.replace(tmp, path)
+
+
+def load_structure(path, key=None):
+    """Reads a Structure written by save_structure; None if the file is missing,
+    of another format or (with ``key``) built from other input."""
+    import os
+
+    if not os.path.exists(path):
+        return None
+    with np.load(path) as d:
+        if str(d["_format"]) != _FORMAT or (key is not None and str(d["_key"]) != key):
+            return None
+        n, cand, cost, nnz_a = (int(v) for v in d["_meta"])
+        arrays = {name: d[name] for name, _, _ in _FIELDS}
+    return Structure(n=n, n_candidates=cand, tree_cost=cost, nnz_a=nnz_a, **arrays)
+
+
+def structure_key(row, col, n_rows, alpha):
+    """SHA-1 of the edge list, the row count and alpha: names a cached structure."""
+    import hashlib
+
+    h = hashlib.sha1()
+    for a in (_as_numpy_i32(row, "src_row_idx"), _as_numpy_i32(col, "src_col_idx")):
+        h.update(np.ascontiguousarray(a).view(np.uint8))
+    h.update(f"|{int(n_rows)}|{int(alpha)}|{_FORMAT}".encode())
+    return h.hexdigest()
+
+
+def build_cached(row, col, n_rows, alpha=0, cache_dir=None, n_threads=0):
+    """build() through an on-disk cache in ``cache_dir`` (none: plain build).
+    Construction dominates set-up on large graphs (tens of seconds at millions
+    of rows); the cache holds the six arrays of init plus the CSR form."""
+    if not cache_dir:
+        return build(row, col, n_rows, alpha, n_threads)
+    import os
+
+    os.makedirs(cache_dir, exist_ok=True)
+    key = structure_key(row, col, n_rows, alpha)
+    path = os.path.join(cache_dir, f"cbm-{key[:20]}.npz")
+    s = load_structure(path, key)
+    if s is None:
+        s = build(row, col, n_rows, alpha, n_threads)
+        save_structure(path, s, key)
+    return s

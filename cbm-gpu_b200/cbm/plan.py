@@ -170,6 +170,18 @@ class Plan:
                                   ws.data_ptr(), ws.numel(), _stream(self.device))
         _lib.check(rc, "cbm_matmul")
 
+    def matmul_gin(self, x, y, epsilon):
+        """y <- A x + (1 + epsilon) x (GIN aggregation) on the current stream."""
+        xdt, ldx = self._operand(x, self.n_cols, "rhs")
+        ydt, ldy = self._operand(y, self.n_rows, "res")
+        if x.shape[1] != y.shape[1]:
+            raise RuntimeError(f"rhs has {x.shape[1]} columns, res {y.shape[1]}")
+        cols = int(x.shape[1])
+        ws = self.workspace(_lib.OP_GIN, cols, xdt, ydt, False)
+        rc = self._lib.cbm_matmul_gin(self._h, float(epsilon), x.data_ptr(), xdt, ldx, y.data_ptr(), ydt, ldy, cols,
+                                      ws.data_ptr(), ws.numel(), _stream(self.device))
+        _lib.check(rc, "cbm_matmul_gin")
+
     def matmul_host(self, op, x, y, slab_cols=64):
         """y <- op(A) x with x and y in host memory (pinned for full-speed copies):
         column slabs are copied in, multiplied and copied out on overlapping

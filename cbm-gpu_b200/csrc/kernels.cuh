@@ -99,6 +99,12 @@ struct FwdArgs {
   int32_t comp_read0;
   float* pcomp;        // [n_internal, ldp] residual rows of internal nodes
   int32_t tma_rb;      // TMA variant: bytes of one gathered row (nvec * 16)
+  // GIN form (register kernel only): Y[v] = (A X)[v] + gin_scale * X[v]
+  // (gin_scale = 1 + epsilon), the self term added in the final store only;
+  // internal nodes then keep their (A X) rows in pstate for their children,
+  // as with BF16 Y
+  int32_t gin;
+  float gin_scale;
   long long timeout_ns;
 };
 
@@ -344,6 +350,20 @@ __device__ __forceinline__ void fwd_chunk(const FwdArgs& a, int k, unsigned epoc
   if (tl == 0) st_release(a.chunk_flag + k, epoch);
 }
 
+// out = gin_scale * X[node] + acc (one rounding) for the GIN form, else acc
+template <typename XT, int V>
+__device__ __forceinline__ void gin_self(const FwdArgs& a, int node, int vi, const float (&acc)[V], float (&out)[V]) {
+  if (a.gin) {
+    float xs[V];
+    Vec<XT, V>::load(static_cast<const XT*>(a.x) + (int64_t)node * a.ldx + (int64_t)vi * V, xs);
+#pragma unroll
+    for (int q = 0; q < V; ++q) out[q] = fmaf(a.gin_scale, xs[q], acc[q]);
+  } else {
+#pragma unroll
+    for (int q = 0; q < V; ++q) out[q] = acc[q];
+  }
+}
+
 // s + e == a + b exactly (Knuth's TwoSum; explicit roundings, no contraction)
 __device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
   s = __fadd_rn(a, b);
@@ -401,7 +421,7 @@ __device__ __forceinline__ void fwd_row(const FwdArgs& a, int item, unsigned epo
       const int vi = tl + v * TL;
       if (vi < a.nvec) {
         float yp[V];
-        if constexpr (sizeof(YT) == 4) {
+        if (sizeof(YT) == 4 && !a.gin) {
           load_y_cg<YT, V>(static_cast<const YT*>(a.y) + (int64_t)p * a.ldy + (int64_t)vi * V, yp);
         } else {
           load_f32_cg<V>(a.pstate + (int64_t)ps * a.ldp + vi * V, yp);
@@ -466,10 +486,14 @@ __device__ __forceinline__ void fwd_row(const FwdArgs& a, int item, unsigned epo
 #pragma unroll
   for (int v = 0; v < VPL; ++v) {
     const int vi = tl + v * TL;
-    if (vi < a.nvec) store_vec<YT, V>(yrow + (int64_t)vi * V, acc[v]);
+    if (vi < a.nvec) {
+      float out[V];
+      gin_self<XT, V>(a, node, vi, acc[v], out);
+      store_vec<YT, V>(yrow + (int64_t)vi * V, out);
+    }
   }
   if (internal) {
-    if constexpr (sizeof(YT) != 4) {
+    if (sizeof(YT) != 4 || a.gin) {
       float* srow = a.pstate + (int64_t)a.self_slot[item] * a.ldp;
 #pragma unroll
       for (int v = 0; v < VPL; ++v) {
@@ -987,7 +1011,7 @@ __device__ __forceinline__ void stream_pass_tma(const CUtensorMap* tmap, int rb,
 // per-thread cp.async ring of stream_pass (tmap unused).
 template <typename XT, typename YT, int TL, int VPL, int V, int S, int BLOCK, bool TMA = false>
 __global__ void __launch_bounds__(BLOCK) fwd_stream_kernel(const FwdArgs a, const __grid_constant__ CUtensorMap tmap) {
-  extern __shared__ __align__(1024) uint4 ring[];
+  extern __shared__ __align__(128) uint4 ring[];
   const int lane = threadIdx.x & 31;
   const int team = lane / TL;
   const int tl = lane & (TL - 1);

@@ -482,7 +482,6 @@ extern "C" {
 int64_t cbm_plan_workspace_bytes(const cbm_plan* P, int32_t op, int64_t n_cols, int32_t x_dtype, int32_t y_dtype,
                                  int32_t adjoint) {
   if (!P || n_cols < 0) return -1;
-  (void)op;
   const int vv = x_dtype == CBM_BF16 ? 8 : 4;
   const int64_t cols = std::min<int64_t>(n_cols, block_cols(vv));
   const int64_t ldp = round4(cols);
@@ -493,7 +492,7 @@ int64_t cbm_plan_workspace_bytes(const cbm_plan* P, int32_t op, int64_t n_cols, 
     const int64_t t_chunks = P->adj_built ? P->n_t_chunks : (2 * P->nnz / P->chunk_nnz + 1);
     rows = P->n_internal + t_chunks + (P->adj_built ? P->n_rev_chunks : P->n_internal);
   } else {
-    rows = P->n_chunks + (y_dtype == CBM_BF16 ? P->n_internal : 0) +
+    rows = P->n_chunks + ((y_dtype == CBM_BF16 || op == CBM_OP_GIN) ? P->n_internal : 0) +
            (comp_active(P, x_dtype) ? P->n_internal : 0);
   }
   return align256(rows * ldp * 4) + 256;
@@ -525,7 +524,24 @@ int cbm_plan_debug_set_parent(cbm_plan* P, int64_t item, int32_t parent_node, vo
 
 int cbm_matmul(cbm_plan* P, int32_t op, const void* x, int32_t xdt, int64_t ldx, void* y, int32_t ydt, int64_t ldy,
                int64_t n_cols, void* ws, int64_t ws_bytes, void* stream) {
-  if (!P || op < CBM_OP_AX || op > CBM_OP_DAD_ADD || n_cols < 0) return CBM_ERR_INVALID;
+  if (op == CBM_OP_GIN) return CBM_ERR_INVALID;  // needs epsilon: cbm_matmul_gin
+  return cbm::matmul_impl(P, op, 0.f, x, xdt, ldx, y, ydt, ldy, n_cols, ws, ws_bytes, stream);
+}
+
+int cbm_matmul_gin(cbm_plan* P, float epsilon, const void* x, int32_t xdt, int64_t ldx, void* y, int32_t ydt,
+                   int64_t ldy, int64_t n_cols, void* ws, int64_t ws_bytes, void* stream) {
+  if (P && P->n_rows != P->n_cols) return CBM_ERR_SHAPE;  // X[v] must exist for every row v
+  return cbm::matmul_impl(P, CBM_OP_GIN, 1.0f + epsilon, x, xdt, ldx, y, ydt, ldy, n_cols, ws, ws_bytes, stream);
+}
+
+}  // extern "C"
+
+namespace cbm {
+
+int matmul_impl(cbm_plan* P, int32_t op, float gin_scale, const void* x, int32_t xdt, int64_t ldx, void* y,
+                int32_t ydt, int64_t ldy, int64_t n_cols, void* ws, int64_t ws_bytes, void* stream) {
+  if (!P || op < CBM_OP_AX || op > CBM_OP_GIN || n_cols < 0) return CBM_ERR_INVALID;
+  const bool gin = op == CBM_OP_GIN;
   if (!dtype_ok(xdt, ydt)) return CBM_ERR_DTYPE;
   if (n_cols == 0 || P->n_rows == 0) return CBM_OK;
   if (!x || !y) return CBM_ERR_INVALID;
@@ -536,7 +552,8 @@ int cbm_matmul(cbm_plan* P, int32_t op, const void* x, int32_t xdt, int64_t ldx,
   if ((op == CBM_OP_VALUES_ADD || op == CBM_OP_VALUES_RATIO) && xdt != CBM_F32) return CBM_ERR_DTYPE;
   const int64_t need = cbm_plan_workspace_bytes(P, op, n_cols, xdt, ydt, 0);
   const bool comp = comp_active(P, xdt);
-  const bool need_ws = P->n_chunks > 0 || (ydt == CBM_BF16 && P->n_internal > 0) || comp;
+  const bool state_rows = ydt == CBM_BF16 || gin;  // parents' rows come from pstate
+  const bool need_ws = P->n_chunks > 0 || (state_rows && P->n_internal > 0) || comp;
   if (need_ws && (!ws || ws_bytes < need)) return CBM_ERR_WORKSPACE;
   if (ws && reinterpret_cast<uintptr_t>(ws) % 16 != 0) return CBM_ERR_INVALID;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -552,6 +569,7 @@ int cbm_matmul(cbm_plan* P, int32_t op, const void* x, int32_t xdt, int64_t ldx,
       prop = PROP_RATIO;
       break;
     case CBM_OP_DAD_ADD: scale = SCALE_DCOL_DROW; break;
+    case CBM_OP_GIN: scale = P->unit_values ? SCALE_SIGN : SCALE_VALUES; break;
   }
   const Shape sh = pick_shape(xdt, ydt, x, ldx, y, ldy, n_cols);
   for (int64_t c0 = 0; c0 < n_cols; c0 += sh.cb) {
@@ -590,10 +608,12 @@ int cbm_matmul(cbm_plan* P, int32_t op, const void* x, int32_t xdt, int64_t ldx,
     a.ldp = (int32_t)ldp;
     a.partial = static_cast<float*>(ws);
     a.pstate = ws ? static_cast<float*>(ws) + P->n_chunks * ldp : nullptr;
+    a.gin = gin ? 1 : 0;
+    a.gin_scale = gin_scale;
     a.comp_item0 = (int32_t)P->n_items;
     a.comp_read0 = (int32_t)P->n_items;
     if (comp) {
-      a.pcomp = static_cast<float*>(ws) + (P->n_chunks + (ydt == CBM_BF16 ? P->n_internal : 0)) * ldp;
+      a.pcomp = static_cast<float*>(ws) + (P->n_chunks + (state_rows ? P->n_internal : 0)) * ldp;
       a.comp_item0 = (int32_t)P->level_start[P->comp_depth];
       a.comp_read0 = (int32_t)P->level_start[std::min<int64_t>(P->comp_depth + 1, P->levels)];
     }
@@ -611,7 +631,9 @@ int cbm_matmul(cbm_plan* P, int32_t op, const void* x, int32_t xdt, int64_t ldx,
     a.hints = P->hot_rows > 0 ? 1 : 0;
     a.timeout_ns = P->timeout_ns;
     int s_team = 0, s_vpl = 0;
-    const bool staged = sh.vec && P->variant != CBM_VARIANT_REGISTER &&
+    // the GIN form runs on the register kernel (its self term and state rows
+    // stay out of the staged kernel's registers)
+    const bool staged = sh.vec && !gin && P->variant != CBM_VARIANT_REGISTER &&
                         staged_shape(nvec, sh.v, P->staged_team, &s_team, &s_vpl);
     const bool tma = staged && P->variant == CBM_VARIANT_TMA && tma_shape(nvec, sh.v, s_team, s_vpl);
     int rc;
@@ -633,6 +655,10 @@ int cbm_matmul(cbm_plan* P, int32_t op, const void* x, int32_t xdt, int64_t ldx,
   }
   return CBM_OK;
 }
+
+}  // namespace cbm
+
+extern "C" {
 
 int cbm_matmul_host(cbm_plan* P, int32_t op, const void* x_host, int32_t xdt, int64_t ldx_host, void* y_host,
                     int32_t ydt, int64_t ldy_host, int64_t n_cols, int64_t slab_cols, void* x_dev, void* y_dev,

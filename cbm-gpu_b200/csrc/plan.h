@@ -96,4 +96,6 @@ int build_layout(cbm_plan* P, cudaStream_t st);
 int rebuild_adjoint_chunks(cbm_plan* P, cudaStream_t st);
 void release_pipeline(cbm_plan* P);
 int transpose_on_device(cbm_plan* P, cudaStream_t st);
+int matmul_impl(cbm_plan* P, int32_t op, float gin_scale, const void* x, int32_t xdt, int64_t ldx, void* y,
+                int32_t ydt, int64_t ldy, int64_t n_cols, void* ws, int64_t ws_bytes, void* stream);
 }  // namespace cbm

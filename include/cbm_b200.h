@@ -61,8 +61,10 @@ enum {
   CBM_OP_DADX = 2,        /* Y = D^-1/2 A D^-1/2 X (signs, D[col]*D[row], ratio)  */
   CBM_OP_VALUES_ADD = 3,  /* Y = Dv X; Y[v] += Y[u]            (matmul_AX_ADX)   */
   CBM_OP_VALUES_RATIO = 4, /* Y = Dv X; Y[v] += Y[u]*m[v]/m[u]  (matmul_DAX_DADX) */
-  CBM_OP_DAD_ADD = 5       /* entries s*m[col]*m[row], Y[v] += Y[u]: what matmul_AX_ADX
+  CBM_OP_DAD_ADD = 5,      /* entries s*m[col]*m[row], Y[v] += Y[u]: what matmul_AX_ADX
                               computes on the values cbm4dad prepares                 */
+  CBM_OP_GIN = 6           /* Y = A X + (1 + eps) X: cbm_matmul_gin only (its workspace
+                              query uses this op)                                      */
 };
 
 /* ---- construction (host, OpenMP) ----------------------------------------- */
@@ -172,6 +174,17 @@ int64_t cbm_plan_workspace_bytes(const cbm_plan* plan, int32_t op, int64_t n_col
 int cbm_matmul(cbm_plan* plan, int32_t op, const void* x, int32_t x_dtype, int64_t ldx, void* y,
                int32_t y_dtype, int64_t ldy, int64_t n_cols, void* workspace, int64_t workspace_bytes,
                void* stream);
+
+/* GIN aggregation Y = A X + (1 + epsilon) X on the CBM product, with the self
+ * term fused into the final store (the parent rows propagated down the tree
+ * are the A X rows, kept in the workspace).  Square A; X and Y as for
+ * cbm_matmul; workspace: cbm_plan_workspace_bytes(plan, CBM_OP_GIN, ...).
+ * Each element is fma(1 + epsilon, X[v], (A X)[v]).
+ * Replaces s_spmm_update_add_csr_int32 (cbm/cbm_extensions.cpp:498-591), the
+ * reference's CPU-only GIN form (its MKL SpMM + update + cblas_saxpy). */
+int cbm_matmul_gin(cbm_plan* plan, float epsilon, const void* x, int32_t x_dtype, int64_t ldx, void* y,
+                   int32_t y_dtype, int64_t ldy, int64_t n_cols, void* workspace, int64_t workspace_bytes,
+                   void* stream);
 
 /* Y = op(A) X for operands in host memory (page-locked for full-speed
  * copies): X is copied in and Y out in column slabs of slab_cols columns (0:

@@ -16,6 +16,9 @@
  *                         chosen in-edge per node (cbm/cbm_extensions.cpp:191-299)
  *   oracle_spmm_update    CSR SpMM then branch-serial Y[dst] += Y[src]
  *                         (cbm/cbm_extensions.cpp:351-444, cbm/cbm.cu:25-57)
+ *   oracle_spmm_update_add
+ *                         ... then Y += (1 + eps) X, the GIN form
+ *                         (cbm/cbm_extensions.cpp:498-591)
  *   oracle_spmm_fused_update
  *                         ... with Y[dst] += Y[src] * m[dst] / m[src]; mode 0
  *                         evaluates it as the reference GPU kernel does
@@ -284,6 +287,18 @@ void oracle_spmm_update(int64_t n_rows, int64_t c, const int32_t* rp, const int3
                         const int32_t* dst, float* y) {
   csr_spmm_f32(n_rows, c, rp, ci, val, x, y, 0);
   update(c, n_branches, br, src, dst, NULL, 0, y, 0);
+}
+
+/* s_spmm_update_add_csr_int32 (cbm/cbm_extensions.cpp:498-591): the CBM
+ * product, then y += (1 + eps) x over all elements (its cblas_saxpy), taken
+ * here as one fused multiply-add per element. */
+void oracle_spmm_update_add(int64_t n_rows, int64_t c, const int32_t* rp, const int32_t* ci, const float* val,
+                            const float* x, float eps, int64_t n_branches, const int32_t* br, const int32_t* src,
+                            const int32_t* dst, float* y) {
+  csr_spmm_f32(n_rows, c, rp, ci, val, x, y, 0);
+  update(c, n_branches, br, src, dst, NULL, 0, y, 0);
+  const float a = 1.0f + eps;
+  for (int64_t i = 0; i < n_rows * c; ++i) y[i] = fmaf(a, x[i], y[i]);
 }
 
 void oracle_spmm_fused_update(int64_t n_rows, int64_t c, const int32_t* rp, const int32_t* ci, const float* val,

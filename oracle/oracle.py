@@ -142,6 +142,22 @@ def spmm_update(row_ptr, col, val, x, branches, src, dst, parallel=False):
     return y
 
 
+def spmm_update_add(row_ptr, col, val, x, eps, branches, src, dst):
+    """s_spmm_update_add_csr_int32 (cbm/cbm_extensions.cpp:498-591) in fp32: A x + (1 + eps) x."""
+    x = _c(x, np.float32)
+    n = row_ptr.size - 1
+    c = x.shape[1]
+    y = np.empty((n, c), np.float32)
+    rp, ci, va = _c(row_ptr, np.int32), _c(col, np.int32), _c(val, np.float32)
+    br, s, d = _c(branches, np.int32), _c(src, np.int32), _c(dst, np.int32)
+    L = lib()
+    L.oracle_spmm_update_add.restype = None
+    L.oracle_spmm_update_add.argtypes = [i64, i64, vp, vp, vp, vp, C.c_float, i64, vp, vp, vp, vp]
+    L.oracle_spmm_update_add(n, c, rp.ctypes.data, ci.ctypes.data, va.ctypes.data, x.ctypes.data, float(eps),
+                             max(br.size - 1, 0), br.ctypes.data, s.ctypes.data, d.ctypes.data, y.ctypes.data)
+    return y
+
+
 def spmm_fused_update(row_ptr, col, val, x, branches, src, dst, mult, gpu_order=True, parallel=False):
     """matmul_DAX_DADX (cbm/cbm.cu:210-268; gpu_order) or s_spmm_fused_update_csr_int32
     (cbm/cbm_extensions.cpp:593-698) in fp32."""

@@ -184,3 +184,28 @@ def test_thread_count_does_not_change_output(threads):
     b = cbm_mkl_cpp.build(ei[0], ei[1], 500, 2, n_threads=0)
     for f in ("delta_row", "delta_col", "delta_val", "branches", "src", "dst"):
         np.testing.assert_array_equal(getattr(a, f), getattr(b, f))
+
+
+def test_structure_cache_round_trip(tmp_path):
+    """The on-disk structure cache returns exactly what the constructor built,
+    keyed by the edge list and alpha."""
+    from cbm import cbm_mkl_cpp
+    from conftest import near_dup_graph
+
+    ei = near_dup_graph(700, seed=9)
+    s0 = cbm_mkl_cpp.build(ei[0], ei[1], 700, 2)
+    s1 = cbm_mkl_cpp.build_cached(ei[0], ei[1], 700, 2, cache_dir=str(tmp_path))
+    s2 = cbm_mkl_cpp.build_cached(ei[0], ei[1], 700, 2, cache_dir=str(tmp_path))  # from the file
+    files = list(tmp_path.iterdir())
+    assert len(files) == 1
+    for s in (s1, s2):
+        for f in ("delta_row", "delta_col", "delta_val", "branches", "src", "dst", "parent", "csr_ptr", "csr_col",
+                  "csr_val"):
+            np.testing.assert_array_equal(getattr(s, f), getattr(s0, f))
+        assert (s.n, s.tree_cost, s.nnz_a, s.n_candidates) == (s0.n, s0.tree_cost, s0.nnz_a, s0.n_candidates)
+    # another alpha is another entry
+    s3 = cbm_mkl_cpp.build_cached(ei[0], ei[1], 700, 0, cache_dir=str(tmp_path))
+    assert len(list(tmp_path.iterdir())) == 2
+    np.testing.assert_array_equal(s3.csr_col, cbm_mkl_cpp.build(ei[0], ei[1], 700, 0).csr_col)
+    # a file of another format or key is ignored
+    assert cbm_mkl_cpp.load_structure(str(files[0]), key="other") is None
