@@ -90,6 +90,12 @@ struct FwdArgs {
   int32_t rows_per_claim;       // level-0 rows a team takes per claim
   int32_t rows_per_claim_deep;  // rows below level 0 a team takes per claim
   int32_t n_root;               // items [0, n_root) are level 0 (no parent)
+  // staged kernel with several teams per warp: claims of one unit per team,
+  // unit u = items [unit[u], unit[u + 1]) (at most 8), level-0 units balanced
+  // by entries (null, or full-warp teams: claims of rows_per_claim /
+  // rows_per_claim_deep items)
+  const int32_t* unit;
+  int32_t n_units;
   int32_t hints;       // L2 cache policies on (staged kernel)
   // compensated propagation (register kernel, COMP = true): items from
   // comp_item0 on (tree depth >= the plan's threshold) add their parent term
@@ -1090,16 +1096,32 @@ __global__ void __launch_bounds__(BLOCK) fwd_stream_kernel(const FwdArgs a, cons
   const int64_t hi = a.n_items;
   unsigned last = 0;
   for (;;) {
-    const int Rp = last < (unsigned)a.n_root ? a.rows_per_claim : a.rows_per_claim_deep;
-    const int R = Rp < TL ? Rp : TL;
-    unsigned claimed = 0;
-    if (lane == 0) claimed = atomicAdd(&a.qs->next_row, (unsigned)(teams * R));
-    const unsigned base = __shfl_sync(0xffffffffu, claimed, 0);
-    if ((int64_t)base >= hi) break;
-    last = base;
-    const int64_t i0 = (int64_t)base + (int64_t)team * R;
+    // this team's items [i0, i1); base: the first item of the warp's claim
+    int64_t i0, i1;
+    unsigned base;
+    // units pay off where teams share a warp (they step together); a full-warp
+    // team keeps the plain claims (one dependent load fewer per claim)
+    if (TL < 32 && a.unit) {
+      unsigned claimed = 0;
+      if (lane == 0) claimed = atomicAdd(&a.qs->next_row, (unsigned)teams);
+      const unsigned ub = __shfl_sync(0xffffffffu, claimed, 0);
+      if (ub >= (unsigned)a.n_units) break;
+      const unsigned u = ub + team;
+      base = (unsigned)a.unit[ub];
+      i0 = u < (unsigned)a.n_units ? a.unit[u] : hi;
+      i1 = u < (unsigned)a.n_units ? a.unit[u + 1] : hi;
+    } else {
+      const int Rp = last < (unsigned)a.n_root ? a.rows_per_claim : a.rows_per_claim_deep;
+      const int R = Rp < TL ? Rp : TL;
+      unsigned claimed = 0;
+      if (lane == 0) claimed = atomicAdd(&a.qs->next_row, (unsigned)(teams * R));
+      base = __shfl_sync(0xffffffffu, claimed, 0);
+      if ((int64_t)base >= hi) break;
+      last = base;
+      i0 = (int64_t)base + (int64_t)team * R;
+      i1 = (i0 + R < hi) ? i0 + R : hi;
+    }
     {
-      const int64_t i1 = (i0 + R < hi) ? i0 + R : hi;
       const int nit = i0 < hi ? (int)(i1 - i0) : 0;
       const int64_t k0 = nit > 0 ? a.ptr[i0] : 0;
       // item metadata, one item per lane; ends relative to k0

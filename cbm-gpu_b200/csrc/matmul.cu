@@ -621,13 +621,10 @@ int matmul_impl(cbm_plan* P, int32_t op, float gin_scale, const void* x, int32_t
     a.prop_mode = prop;
     a.team = team;
     a.rows_per_claim = P->rows_per_claim;
-    // Rows below level 0 wait on parents claimed just before them; when they
-    // are a large share of the rows, one-row claims keep that chain short.
-    // Otherwise their parents are long finished and larger claims cost less.
-    a.rows_per_claim_deep = P->rows_per_claim_deep > 0
-                                ? P->rows_per_claim_deep
-                                : ((P->n_items - P->n_root) * 4 > P->n_items ? 1 : P->rows_per_claim);
+    a.rows_per_claim_deep = deep_rows_per_claim(P);
     a.n_root = (int32_t)P->n_root;
+    a.unit = P->d_unit;
+    a.n_units = (int32_t)P->n_units;
     a.hints = P->hot_rows > 0 ? 1 : 0;
     a.timeout_ns = P->timeout_ns;
     int s_team = 0, s_vpl = 0;

@@ -190,7 +190,53 @@ int build_layout(cbm_plan* P, cudaStream_t st) {
     P->d_chunk_flag = nullptr;
   }
   // chunk flags restart at 0 while the epoch keeps counting: never equal
+  if ((rc = build_units(P, st))) return rc;
   return cuda_status(cudaStreamSynchronize(st));
+}
+
+// Rows below level 0 wait on parents claimed just before them; when they are a
+// large share of the rows, one-row claims keep that chain short.  Otherwise
+// their parents are long finished and larger claims cost less.
+int32_t deep_rows_per_claim(const cbm_plan* P) {
+  if (P->rows_per_claim_deep > 0) return P->rows_per_claim_deep;
+  return (P->n_items - P->n_root) * 4 > P->n_items ? 1 : P->rows_per_claim;
+}
+
+// Claim units of the staged kernel.  Level-0 items (which wait on nothing) are
+// grouped greedily into runs whose cost reaches rows_per_claim x the mean
+// cost of a level-0 row, at most kMaxUnit items: teams that step together
+// then get similar amounts of work.  A row costs its entries plus 4 (its
+// finishing work); a split row costs its chunk count plus 4 (its entries are
+// summed by chunk teams).  Items below level 0 keep fixed-size claims of
+// deep_rows_per_claim items.
+int build_units(cbm_plan* P, cudaStream_t st) {
+  constexpr int64_t kMaxUnit = 8;  // items held one per lane by the narrowest team
+  free_all(P->unit_bufs);
+  P->d_unit = nullptr;
+  P->n_units = 0;
+  const int64_t n = P->n_items, nr = std::min<int64_t>(P->n_root, n);
+  if (n == 0) return CBM_OK;
+  const int64_t T = P->chunk_nnz;
+  auto cost = [&](int64_t i) {
+    const int64_t len = P->h_ptr[i + 1] - P->h_ptr[i];
+    return (len > T ? (len + T - 1) / T : len) + 4;
+  };
+  double total = 0;
+  for (int64_t i = 0; i < nr; ++i) total += (double)cost(i);
+  const double target = nr > 0 ? P->rows_per_claim * total / (double)nr : 0.0;
+  std::vector<int32_t> unit(1, 0);
+  int64_t i = 0;
+  while (i < nr) {
+    double c = 0;
+    int64_t j = i;
+    while (j < nr && j - i < kMaxUnit && (j == i || c + 0.5 * (double)cost(j) <= target)) c += (double)cost(j++);
+    unit.push_back((int32_t)j);
+    i = j;
+  }
+  const int64_t rd = std::max<int32_t>(1, std::min<int32_t>(deep_rows_per_claim(P), (int32_t)kMaxUnit));
+  for (; i < n; i += rd) unit.push_back((int32_t)std::min(n, i + rd));
+  P->n_units = (int64_t)unit.size() - 1;
+  return dev_upload(&P->d_unit, unit, st, P->unit_bufs);
 }
 
 }  // namespace cbm
@@ -243,6 +289,7 @@ int cbm_plan_create(const int32_t* row_ptr, const int32_t* col_idx, const float*
   cbm_plan* P = new (std::nothrow) cbm_plan();
   if (!P) return CBM_ERR_ALLOC;
   auto fail = [&](int rc) {
+    free_all(P->unit_bufs);
     free_all(P->chunk_bufs);
     free_all(P->bufs);
     delete P;
@@ -386,21 +433,27 @@ int cbm_plan_tune(cbm_plan* P, int32_t chunk_nnz, int32_t rows_per_claim, int32_
                   int32_t variant, int64_t hot_rows, int32_t team, void* stream) {
   if (!P || chunk_nnz < 32 || rows_per_claim < 1 || rows_per_claim > 1024 || hot_rows < 0) return CBM_ERR_INVALID;
   if (rows_per_claim_deep < 0 || rows_per_claim_deep > 1024) return CBM_ERR_INVALID;
+  const bool deep_changed = rows_per_claim_deep != P->rows_per_claim_deep;
   P->rows_per_claim_deep = rows_per_claim_deep;
   if (team != 0 && team != 8 && team != 16 && team != 32) return CBM_ERR_INVALID;
   P->staged_team = team;
   if (variant < CBM_VARIANT_AUTO || variant > CBM_VARIANT_TMA) return CBM_ERR_INVALID;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (cudaStreamSynchronize(st) != cudaSuccess) return CBM_ERR_CUDA;
+  const bool claims_changed = rows_per_claim != P->rows_per_claim;
   P->rows_per_claim = rows_per_claim;
   P->variant = variant;
   if (chunk_nnz != P->chunk_nnz || hot_rows != P->hot_rows) {
     P->chunk_nnz = chunk_nnz;
     P->hot_rows = hot_rows;
-    int rc = build_layout(P, st);
+    int rc = build_layout(P, st);  // rebuilds the units too
     if (rc) return rc;
     rc = rebuild_adjoint_chunks(P, st);
     if (rc) return rc;
+  } else if (claims_changed || deep_changed) {
+    int rc = build_units(P, st);
+    if (rc) return rc;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return CBM_ERR_CUDA;
   }
   return CBM_OK;
 }
@@ -452,6 +505,7 @@ void cbm_plan_destroy(cbm_plan* P) {
   cudaGetDevice(&cur);
   if (cur != P->device) cudaSetDevice(P->device);
   release_pipeline(P);
+  free_all(P->unit_bufs);
   free_all(P->chunk_bufs);
   free_all(P->adj_bufs);
   free_all(P->adj_chunk_bufs);

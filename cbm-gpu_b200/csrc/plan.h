@@ -59,6 +59,10 @@ struct cbm_plan {
   int64_t* d_chunk_beg = nullptr;
   int64_t* d_chunk_end = nullptr;
   unsigned* d_chunk_flag = nullptr;
+  // claim units of the staged kernel (build_units)
+  int64_t n_units = 0;
+  int32_t* d_unit = nullptr;
+  std::vector<void*> unit_bufs;
 
   // adjoint layout (built on first use)
   bool adj_built = false;
@@ -93,6 +97,8 @@ namespace cbm {
 int cuda_status(cudaError_t e);
 void free_all(std::vector<void*>& v);
 int build_layout(cbm_plan* P, cudaStream_t st);
+int build_units(cbm_plan* P, cudaStream_t st);
+int32_t deep_rows_per_claim(const cbm_plan* P);
 int rebuild_adjoint_chunks(cbm_plan* P, cudaStream_t st);
 void release_pipeline(cbm_plan* P);
 int transpose_on_device(cbm_plan* P, cudaStream_t st);
