@@ -379,6 +379,53 @@ def run_precision(args):
     print(json.dumps(line), flush=True)
 
 
+def run_lsh(args):
+    """LSH-clustered form: the rows of the 1,000,000-node power-law graph are
+    clustered by the reference's hierarchical fingerprinting
+    (benchmark/clustering_gpu.py, 4 hash columns, clusters of at most
+    args.max_cluster rows), one CBM forest per cluster in one structure, and
+    D^-1/2 A D^-1/2 X (fp32, 256 columns) runs over all clusters in one launch.
+    Reports the reference's compression figures next to the timing."""
+    from cbm import synthetic
+    from cbm.cbm4dad import cbm4dad
+    from cbm.cluster import cluster_ids, lsh_clusters
+
+    ei, n, spec = load_graph(0, 1)
+    t0 = time.time()
+    cl = lsh_clusters(ei, n, max_cluster_size=args.max_cluster, num_hashes=4)
+    t_cluster = time.time() - t0
+    a = cbm4dad(torch.from_numpy(ei), torch.ones(ei.shape[1]), alpha=spec["alpha"], cache_dir=CACHE,
+                cluster=cluster_ids(cl, n))
+    full = cbm4dad(torch.from_numpy(ei), torch.ones(ei.shape[1]), alpha=spec["alpha"], cache_dir=CACHE)
+    g = torch.Generator(device="cuda").manual_seed(1)
+    x = torch.randn(n, COLS, device="cuda", generator=g)
+    y = torch.empty(n, COLS, device="cuda")
+    ms = _time_events(lambda: a.matmul(x, y), args.steps, args.warmup)
+    ms_full = _time_events(lambda: full.matmul(x, y), args.steps, args.warmup)
+    a.matmul(x, y)
+    st = a.plan.stats
+    b_alg = bytes_alg(n, st["nnz"], st["edges"], st["branches"], COLS)
+    d = dinv_f64(ei, n)
+    sizes = sorted(c.size for c in cl)
+    line = {"metric": "CBM DAD.X GB/s over LSH clusters (algorithmic bytes)", "value": b_alg / (ms * 1e-3) / 1e9,
+            "unit": "GB/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{WORKLOAD} rows in LSH clusters (4 hashes, <= {args.max_cluster} rows), "
+                                   f"one launch", "nodes": n, "cols": COLS, "clusters": len(cl),
+                       "cluster_rows_min_median_max": [sizes[0], sizes[len(sizes) // 2], sizes[-1]],
+                       "clustering_s": t_cluster},
+            "compression": {"nnz_csr": a.structure_stats["nnz_a"], "nnz_cbm": full.structure_stats["nnz_delta"],
+                            "nnz_cbm_clustered": st["nnz"],
+                            "reduction_vs_csr": a.structure_stats["nnz_a"] / st["nnz"],
+                            "reduction_vs_cbm": full.structure_stats["nnz_delta"] / st["nnz"]},
+            "unclustered_ms": ms_full,
+            "roofline": {"bound": "hbm", "achieved": b_alg / (ms * 1e-3) / 1e9, "peak": peaks()[0], "unit": "GB/s",
+                         "frac": b_alg / (ms * 1e-3) / 1e9 / peaks()[0], "peak_kind": peaks()[1]},
+            "error_vs_fp64": fp64_sample_error(ei, n, x, y, rs=d, cs=d)}
+    a.plan.check_device()
+    print(json.dumps(line), flush=True)
+
+
 def config_dict(n, nnz_a, z, e, b, world):
     return {"workload": f"{WORKLOAD}: D^-1/2 A D^-1/2 X fp32, power-law N={n}, alpha=8, C={COLS} per GPU",
             "nodes": n, "nnz_a": nnz_a, "nnz_delta": z, "tree_edges": e, "branches": b, "cols_per_gpu": COLS,
@@ -394,8 +441,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-gcn", action="store_true")
     ap.add_argument("--gcn-only", action="store_true", help="only the GCN timing (one JSON object)")
-    ap.add_argument("--workload", default="headline", choices=["headline", "batch", "precision"],
-                    help="batch / precision: the batching or precision form instead of the headline line")
+    ap.add_argument("--workload", default="headline", choices=["headline", "batch", "precision", "lsh"],
+                    help="batch / precision / lsh: the batching, precision or LSH-clustered form instead of "
+                         "the headline line")
+    ap.add_argument("--max-cluster", type=int, default=100000, help="lsh workload: cluster size bound")
     ap.add_argument("--variant", default="auto", choices=["auto", "register", "staged"])
     ap.add_argument("--chunk-nnz", type=int, default=256)
     ap.add_argument("--rows-per-claim", type=int, default=4)
@@ -426,7 +475,7 @@ def main():
 
     if args.workload != "headline":
         if rank == 0:
-            (run_batch if args.workload == "batch" else run_precision)(args)
+            {"batch": run_batch, "precision": run_precision, "lsh": run_lsh}[args.workload](args)
         return
     if args.gcn_only:
         if rank == 0:

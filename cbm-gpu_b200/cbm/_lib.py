@@ -35,6 +35,7 @@ i64 = C.c_int64
 # (name, restype, argtypes): every exported symbol of include/cbm_b200.h
 SIGNATURES = [
     ("cbm_build", C.c_int, [vp, vp, i64, i64, i64, i32, i32, C.POINTER(vp)]),
+    ("cbm_build_clustered", C.c_int, [vp, vp, i64, i64, i64, vp, i32, i32, C.POINTER(vp)]),
     ("cbm_coalesce", C.c_int, [vp, vp, i64, i64, i32, vp, vp, C.POINTER(i64)]),
     ("cbm_structure_len", i64, [vp, i32]),
     ("cbm_structure_copy", C.c_int, [vp, i32, vp]),

@@ -19,8 +19,8 @@ __all__ = ["cbm4ad"]
 class cbm4ad(cbm4mm):  # noqa: N801
     _op = "adx"
 
-    def __init__(self, edge_index, edge_values, alpha=0, cache_dir=None):
-        super().__init__(edge_index, edge_values, alpha, cache_dir)
+    def __init__(self, edge_index, edge_values, alpha=0, cache_dir=None, cluster=None):
+        super().__init__(edge_index, edge_values, alpha, cache_dir, cluster)
         num_rows = self.deltas.size()[0]
         d = torch.zeros(num_rows, 1, dtype=torch.float32, device="cuda")
         x = torch.ones(num_rows, 1, dtype=torch.float32, device="cuda")

@@ -23,15 +23,18 @@ __all__ = ["cbm4mm"]
 class cbm4mm:  # noqa: N801 (the reference's class name)
     _op = "ax"
 
-    def __init__(self, edge_index, edge_values, alpha=0, cache_dir=None):
-        """cache_dir (an addition): reuse the constructed structure from an
-        on-disk cache keyed by the edge list and alpha (cbm_mkl_cpp.build_cached)."""
+    def __init__(self, edge_index, edge_values, alpha=0, cache_dir=None, cluster=None):
+        """Additions to the reference's arguments: cache_dir reuses the
+        constructed structure from an on-disk cache keyed by the edge list and
+        alpha (cbm_mkl_cpp.build_cached); cluster (int32 per row, e.g.
+        cbm.cluster.cluster_ids of LSH clusters) restricts every row's parent
+        to its own cluster: the reference's per-cluster CBMs as one operator."""
         if edge_index.numel() == 0:
             raise RuntimeError("edge_index is empty")
         num_rows = int(max(edge_index[0].max(), edge_index[1].max())) + 1
         if isinstance(edge_values, torch.Tensor) and edge_values.dtype != torch.float32:
             raise RuntimeError('"src_values" is not a tensor of type "torch::kFloat32"')
-        s = cbm_mkl.build_cached(edge_index[0], edge_index[1], num_rows, alpha, cache_dir)
+        s = cbm_mkl.build_cached(edge_index[0], edge_index[1], num_rows, alpha, cache_dir, cluster=cluster)
         self.structure_stats = {"nnz_a": s.nnz_a, "nnz_delta": int(s.csr_col.size), "edges": int(s.src.size),
                                 "branches": int(s.branches.size) - 1, "candidates": s.n_candidates}
         self.deltas = torch.sparse_csr_tensor(

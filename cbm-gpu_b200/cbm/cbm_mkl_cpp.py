@@ -74,8 +74,10 @@ def _as_numpy_i32(t, name):
     return np.ascontiguousarray(a)
 
 
-def build(row, col, n_rows, alpha=0, n_threads=0, exhaustive=False):
-    """Runs the constructor on COO indices (int32) and returns a Structure."""
+def build(row, col, n_rows, alpha=0, n_threads=0, exhaustive=False, cluster=None):
+    """Runs the constructor on COO indices (int32) and returns a Structure.
+    cluster (int32 [n_rows], optional): restrict every row's parent to its own
+    cluster (cbm_build_clustered)."""
     lib = _lib.load()
     row = _as_numpy_i32(row, "src_row_idx")
     col = _as_numpy_i32(col, "src_col_idx")
@@ -83,8 +85,16 @@ def build(row, col, n_rows, alpha=0, n_threads=0, exhaustive=False):
         raise RuntimeError("row and column index tensors must be 1-D and of equal length")
     n_rows = int(n_rows)
     h = C.c_void_p()
-    rc = lib.cbm_build(row.ctypes.data, col.ctypes.data, row.size, n_rows, int(alpha), int(n_threads),
-                       _lib.BUILD_EXHAUSTIVE if exhaustive else 0, C.byref(h))
+    flags = _lib.BUILD_EXHAUSTIVE if exhaustive else 0
+    if cluster is None:
+        rc = lib.cbm_build(row.ctypes.data, col.ctypes.data, row.size, n_rows, int(alpha), int(n_threads), flags,
+                           C.byref(h))
+    else:
+        cl = np.ascontiguousarray(cluster, dtype=np.int32)
+        if cl.shape != (n_rows,):
+            raise RuntimeError(f"cluster must hold one id per row ({n_rows}), got {cl.shape}")
+        rc = lib.cbm_build_clustered(row.ctypes.data, col.ctypes.data, row.size, n_rows, int(alpha),
+                                     cl.ctypes.data, int(n_threads), flags, C.byref(h))
     _lib.check(rc, "cbm_build")
     try:
         out = {}
@@ -145,30 +155,34 @@ def load_structure(path, key=None):
     return Structure(n=n, n_candidates=cand, tree_cost=cost, nnz_a=nnz_a, **arrays)
 
 
-def structure_key(row, col, n_rows, alpha):
-    """SHA-1 of the edge list, the row count and alpha: names a cached structure."""
+def structure_key(row, col, n_rows, alpha, cluster=None):
+    """SHA-1 of the edge list, the row count, alpha (and the cluster ids): names
+    a cached structure."""
     import hashlib
 
     h = hashlib.sha1()
-    for a in (_as_numpy_i32(row, "src_row_idx"), _as_numpy_i32(col, "src_col_idx")):
+    parts = [_as_numpy_i32(row, "src_row_idx"), _as_numpy_i32(col, "src_col_idx")]
+    if cluster is not None:
+        parts.append(np.ascontiguousarray(cluster, dtype=np.int32))
+    for a in parts:
         h.update(np.ascontiguousarray(a).view(np.uint8))
     h.update(f"|{int(n_rows)}|{int(alpha)}|{_FORMAT}".encode())
     return h.hexdigest()
 
 
-def build_cached(row, col, n_rows, alpha=0, cache_dir=None, n_threads=0):
+def build_cached(row, col, n_rows, alpha=0, cache_dir=None, n_threads=0, cluster=None):
     """build() through an on-disk cache in ``cache_dir`` (none: plain build).
     Construction dominates set-up on large graphs (tens of seconds at millions
     of rows); the cache holds the six arrays of init plus the CSR form."""
     if not cache_dir:
-        return build(row, col, n_rows, alpha, n_threads)
+        return build(row, col, n_rows, alpha, n_threads, cluster=cluster)
     import os
 
     os.makedirs(cache_dir, exist_ok=True)
-    key = structure_key(row, col, n_rows, alpha)
+    key = structure_key(row, col, n_rows, alpha, cluster)
     path = os.path.join(cache_dir, f"cbm-{key[:20]}.npz")
     s = load_structure(path, key)
     if s is None:
-        s = build(row, col, n_rows, alpha, n_threads)
+        s = build(row, col, n_rows, alpha, n_threads, cluster=cluster)
         save_structure(path, s, key)
     return s

@@ -549,6 +549,11 @@ extern "C" {
 
 int cbm_build(const int32_t* row, const int32_t* col, int64_t nnz, int64_t n_rows, int64_t alpha,
               int32_t n_threads, int32_t flags, cbm_structure** out) {
+  return cbm_build_clustered(row, col, nnz, n_rows, alpha, nullptr, n_threads, flags, out);
+}
+
+int cbm_build_clustered(const int32_t* row, const int32_t* col, int64_t nnz, int64_t n_rows, int64_t alpha,
+                        const int32_t* cluster, int32_t n_threads, int32_t flags, cbm_structure** out) {
   if (!out) return CBM_ERR_INVALID;
   *out = nullptr;
   if (n_rows < 0 || nnz < 0 || n_rows >= INT32_MAX || (nnz > 0 && (!row || !col))) return CBM_ERR_INVALID;
@@ -562,6 +567,13 @@ int cbm_build(const int32_t* row, const int32_t* col, int64_t nnz, int64_t n_row
     s->nnz_a = (int64_t)a.idx.size();
     std::vector<Pair> pairs = (flags & CBM_BUILD_EXHAUSTIVE) ? candidate_pairs_exhaustive(a, alpha, n_threads)
                                                               : candidate_pairs(a, alpha, n_threads);
+    // clustered: a row's parent may only be a row of its own cluster (the
+    // per-cluster CBMs of the reference's LSH clustering, as one forest)
+    if (cluster) {
+      pairs.erase(std::remove_if(pairs.begin(), pairs.end(),
+                                 [&](const Pair& p) { return cluster[p.lo] != cluster[p.hi]; }),
+                  pairs.end());
+    }
     // candidate list in the reference's order
     Arb g;
     g.from.reserve(n + 2 * pairs.size());

@@ -77,6 +77,14 @@ enum { CBM_BUILD_EXHAUSTIVE = 1 }; /* every pair sharing a column (for checks) *
 int cbm_build(const int32_t* row, const int32_t* col, int64_t nnz, int64_t n_rows, int64_t alpha,
               int32_t n_threads, int32_t flags, cbm_structure** out);
 
+/* cbm_build with every row's parent restricted to rows of the same cluster
+ * (cluster: int32 [n_rows], any ids): the forest is the union of the
+ * per-cluster CBMs that the reference's LSH clustering builds one by one
+ * (benchmark/clustering_gpu.py:184-195, cbm4mm per cluster), so one plan and
+ * one launch serve every cluster.  NULL cluster = cbm_build. */
+int cbm_build_clustered(const int32_t* row, const int32_t* col, int64_t nnz, int64_t n_rows, int64_t alpha,
+                        const int32_t* cluster, int32_t n_threads, int32_t flags, cbm_structure** out);
+
 /* COO -> CSR with sorted, unique columns per row, the canonical form the
  * constructor works on (the reference's mkl_sparse_convert_csr,
  * cbm/cbm_extensions.cpp:70-98).  flags: CBM_COALESCE_SYMMETRIZE adds every
