@@ -490,7 +490,13 @@ def main():
     # weak scaling: rank r owns columns [c0, c1) of a [N, COLS * world] X and Y
     c0, c1 = column_shard(COLS * world, rank, world)
     assert c1 - c0 == COLS
+    # rank 0 constructs the CBM into the cache first; the others then load it
+    # (every rank takes the one barrier)
+    if world > 1 and rank != 0:
+        torch.distributed.barrier()
     a = cbm4dad(torch.from_numpy(ei), torch.ones(ei.shape[1]), alpha=spec["alpha"], cache_dir=CACHE)
+    if world > 1 and rank == 0:
+        torch.distributed.barrier()
     a.plan.tune(chunk_nnz=args.chunk_nnz, rows_per_claim=args.rows_per_claim, variant=args.variant,
                 hot_rows=args.hot_rows, team=args.team)
     st = a.plan.stats
