@@ -350,13 +350,20 @@ def run_precision(args):
     else:
         ei, n, spec = synthetic.workload("powerlaw-2.4m")
     a = cbm4ad(torch.from_numpy(ei), torch.ones(ei.shape[1]), alpha=spec["alpha"], cache_dir=CACHE)
-    a.plan.tune(chunk_nnz=args.chunk_nnz, rows_per_claim=args.rows_per_claim, variant=args.variant,
-                hot_rows=args.hot_rows, team=args.team)
     setup_s = time.time() - t0
     g = torch.Generator(device="cuda").manual_seed(2)
     x32 = torch.randn(n, 128, device="cuda", generator=g)
     x = x32.to(torch.bfloat16)
     y = torch.empty(n, 128, device="cuda")
+    if args.no_autotune:
+        a.plan.tune(chunk_nnz=args.chunk_nnz, rows_per_claim=args.rows_per_claim, variant=args.variant,
+                    hot_rows=args.hot_rows, team=args.team)
+        tuned = None
+    else:
+        from cbm.tune import autotune
+
+        tuned = autotune(a.plan, "adx", x, y, space={"chunk_nnz": [256, 512], "rows_per_claim": [2, 4, 8],
+                                                     "variant": ["auto", "register", "tma"]})
     ms = _time_events(lambda: a.matmul(x, y), args.steps, args.warmup)
     dinv = dinv_f64(ei, n)
     err = {"product": fp64_sample_error(ei, n, x, y, cs=dinv),
@@ -374,6 +381,7 @@ def run_precision(args):
             "roofline": {"bound": "hbm", "achieved": b_alg / (ms * 1e-3) / 1e9, "peak": peaks()[0], "unit": "GB/s",
                          "frac": b_alg / (ms * 1e-3) / 1e9 / peaks()[0], "peak_kind": peaks()[1]},
             "plan": st,
+            "autotune_best": {"config": tuned[0][0], "ms": tuned[0][1]} if tuned else None,
             "error_vs_fp64": err}
     a.plan.check_device()
     print(json.dumps(line), flush=True)
@@ -452,6 +460,7 @@ def main():
     ap.add_argument("--hot-rows", type=int, default=65536)
     ap.add_argument("--slab-cols", type=int, default=64, help="column slab of the host-operand product (e2e)")
     ap.add_argument("--prec-nodes", type=int, default=0, help="precision workload at this many nodes (same law)")
+    ap.add_argument("--no-autotune", action="store_true", help="precision workload: the given knobs, no autotuning")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
