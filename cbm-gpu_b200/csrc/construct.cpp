@@ -38,6 +38,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -554,6 +556,10 @@ int cbm_build(const int32_t* row, const int32_t* col, int64_t nnz, int64_t n_row
 
 int cbm_build_clustered(const int32_t* row, const int32_t* col, int64_t nnz, int64_t n_rows, int64_t alpha,
                         const int32_t* cluster, int32_t n_threads, int32_t flags, cbm_structure** out) {
+  nvtxRangePushA("cbm_build");
+  struct Pop {
+    ~Pop() { nvtxRangePop(); }
+  } pop;
   if (!out) return CBM_ERR_INVALID;
   *out = nullptr;
   if (n_rows < 0 || nnz < 0 || n_rows >= INT32_MAX || (nnz > 0 && (!row || !col))) return CBM_ERR_INVALID;

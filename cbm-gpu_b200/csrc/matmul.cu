@@ -393,6 +393,7 @@ int rebuild_adjoint_chunks(cbm_plan* P, cudaStream_t st) {
 // on the device, transpose.cu), built once per plan.
 int build_adjoint(cbm_plan* P, cudaStream_t st) {
   if (P->adj_built) return CBM_OK;
+  CbmRange range("cbm build_adjoint");
   if (P->n_rows >= (int64_t)kInternalBit || P->n_cols >= (int64_t)kInternalBit) return CBM_ERR_INVALID;
   const int64_t n = P->n_rows;
   // children lists, by parent
@@ -540,6 +541,7 @@ namespace cbm {
 
 int matmul_impl(cbm_plan* P, int32_t op, float gin_scale, const void* x, int32_t xdt, int64_t ldx, void* y,
                 int32_t ydt, int64_t ldy, int64_t n_cols, void* ws, int64_t ws_bytes, void* stream) {
+  CbmRange range("cbm_matmul");
   if (!P || op < CBM_OP_AX || op > CBM_OP_GIN || n_cols < 0) return CBM_ERR_INVALID;
   const bool gin = op == CBM_OP_GIN;
   if (!dtype_ok(xdt, ydt)) return CBM_ERR_DTYPE;
@@ -660,6 +662,7 @@ extern "C" {
 int cbm_matmul_host(cbm_plan* P, int32_t op, const void* x_host, int32_t xdt, int64_t ldx_host, void* y_host,
                     int32_t ydt, int64_t ldy_host, int64_t n_cols, int64_t slab_cols, void* x_dev, void* y_dev,
                     void* ws, int64_t ws_bytes, void* stream) {
+  CbmRange range("cbm_matmul_host");
   if (!P || n_cols < 0 || slab_cols < 0) return CBM_ERR_INVALID;
   if (!dtype_ok(xdt, ydt)) return CBM_ERR_DTYPE;
   if (n_cols == 0 || P->n_rows == 0) return CBM_OK;
@@ -719,6 +722,7 @@ int cbm_plan_prepare_adjoint(cbm_plan* P, void* stream) {
 
 int cbm_matmul_adjoint(cbm_plan* P, int32_t op, const void* g, int32_t gdt, int64_t ldg, void* dx, int32_t ddt,
                        int64_t lddx, int64_t n_cols, void* ws, int64_t ws_bytes, void* stream) {
+  CbmRange range("cbm_matmul_adjoint");
   if (!P || op < CBM_OP_AX || op > CBM_OP_DADX || n_cols < 0) return CBM_ERR_INVALID;
   if (!dtype_ok(gdt, ddt)) return CBM_ERR_DTYPE;
   if (n_cols == 0 || P->n_rows == 0 || P->n_cols == 0) return CBM_OK;

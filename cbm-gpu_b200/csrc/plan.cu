@@ -114,6 +114,7 @@ int validate_structure(const int32_t* rp, const int32_t* ci, int64_t n_rows, int
 // longer rows have no entries there and are summed from c_ent in chunks of
 // chunk_nnz entries.
 int build_layout(cbm_plan* P, cudaStream_t st) {
+  CbmRange range("cbm build_layout");
   free_all(P->chunk_bufs);
   const int64_t n = P->n_items;
   const int64_t T = P->chunk_nnz;
@@ -210,6 +211,7 @@ int32_t deep_rows_per_claim(const cbm_plan* P) {
 // summed by chunk teams).  Items below level 0 keep fixed-size claims of
 // deep_rows_per_claim items.
 int build_units(cbm_plan* P, cudaStream_t st) {
+  CbmRange range("cbm build_units");
   constexpr int64_t kMaxUnit = 8;  // items held one per lane by the narrowest team
   free_all(P->unit_bufs);
   P->d_unit = nullptr;
@@ -278,6 +280,7 @@ int cbm_plan_create(const int32_t* row_ptr, const int32_t* col_idx, const float*
                     int64_t n_cols, int64_t nnz, const int32_t* branches, int64_t n_branch_offsets,
                     const int32_t* src, const int32_t* dst, int64_t n_edges, const float* multipliers,
                     int32_t input_kind, void* stream, cbm_plan** out) {
+  CbmRange range("cbm_plan_create");
   if (!out) return CBM_ERR_INVALID;
   *out = nullptr;
   if (n_rows < 0 || n_cols < 0 || nnz < 0 || n_edges < 0 || n_branch_offsets < 0) return CBM_ERR_INVALID;

@@ -4,9 +4,20 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <vector>
 
 #include "kernels.cuh"
+
+// NVTX range over a host-side phase (plan set-up, launches, layouts): named
+// spans in an Nsight timeline; a few nanoseconds when no tool is attached.
+struct CbmRange {
+  explicit CbmRange(const char* name) { nvtxRangePushA(name); }
+  ~CbmRange() { nvtxRangePop(); }
+  CbmRange(const CbmRange&) = delete;
+  CbmRange& operator=(const CbmRange&) = delete;
+};
 
 struct cbm_plan {
   int device = 0;

@@ -75,6 +75,7 @@ int bits_for(int64_t x) {
 // Column pointers (into h_t_ptr, on the host too: the chunk tables need them)
 // and the entry words (P->d_t_ptr, P->d_t_ent, owned by adj_bufs).
 int transpose_on_device(cbm_plan* P, cudaStream_t st) {
+  CbmRange range("cbm transpose_on_device");
   const int64_t n = P->n_items, z = P->nnz, nc = P->n_cols;
   std::vector<void*> tmp;
   auto done = [&](int rc) {

@@ -176,8 +176,9 @@ int64_t cbm_plan_workspace_bytes(const cbm_plan* plan, int32_t op, int64_t n_col
 /* Y = op(A) X.  x: [n_rows, n_cols] row-major with leading dimension ldx, y
  * likewise with ldy; both device memory, not overlapping.  workspace: device
  * scratch of at least cbm_plan_workspace_bytes() bytes.  Allocates nothing,
- * launches one kernel on `stream`, does not synchronise. Calls on one plan must
- * be ordered (one stream, or events): they share the plan's queue state.
+ * launches one kernel on `stream` per block of up to 1,024 (FP32 X) or 2,048
+ * (BF16 X) columns, does not synchronise.  Calls on one plan must be ordered
+ * (one stream, or events): they share the plan's queue state.
  * Replaces matmul_AX_ADX / matmul_DAX_DADX (cbm/cbm.cu:150-268). */
 int cbm_matmul(cbm_plan* plan, int32_t op, const void* x, int32_t x_dtype, int64_t ldx, void* y,
                int32_t y_dtype, int64_t ldy, int64_t n_cols, void* workspace, int64_t workspace_bytes,
