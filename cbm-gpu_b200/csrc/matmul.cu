@@ -673,8 +673,10 @@ int cbm_matmul_host(cbm_plan* P, int32_t op, const void* x_host, int32_t xdt, in
   int64_t w = slab_cols == 0 ? n_cols : std::min(slab_cols, n_cols);
   const int64_t unit = 16 / std::min(xs, ys);
   if (w < n_cols && w % unit != 0) w = std::min(n_cols, (w + unit - 1) / unit * unit);
-  // slab boundaries: w columns each, the last one the remainder (slabs narrower
-  // than 256 bytes make the strided copies slow, so they are not tapered)
+  // slab boundaries: w columns each, the last one the remainder.  Narrower
+  // first or last slabs (to shorten the copy-in that opens the pipeline and
+  // the copy-out that closes it) measured slower on B200: strided copies of
+  // 128-byte pieces lose much of their rate while the other direction runs.
   std::vector<int64_t> bounds(1, 0);
   while (n_cols - bounds.back() > w) bounds.push_back(bounds.back() + w);
   bounds.push_back(n_cols);
