@@ -772,7 +772,10 @@ int cbm_matmul_adjoint(cbm_plan* P, int32_t op, const void* g, int32_t gdt, int6
       r.ldp = (int32_t)ldp;
       r.nvec = (int32_t)nvec;
       r.team = team;
-      r.rows_per_claim = P->rows_per_claim;
+      // every reverse item waits on its children, claimed just before it: one
+      // item per claim keeps a wait from holding up the claim's other items
+      // (measured on the 170K-node GCN graph: 0.42 -> 0.26 ms at 40 columns)
+      r.rows_per_claim = 1;
       r.timeout_ns = P->timeout_ns;
       if ((rc = launch_rev(P, r, gdt, sh.vec, vpl, st))) return rc;
     }
