@@ -12,7 +12,8 @@ reads mca_branches[B + 1], one element past the tensor.  The tensor handed to
 it here is a view of a buffer with one more element equal to the edge count,
 so that read finds an empty range.
 
-Set CBM_REF_TIMING=1 to also time both paths on the 1M-node DAD workload.
+Set CBM_REF_TIMING=1 to also time both paths on the 1M-node DAD workload
+(CBM_REF_TIMING_OUT=path also writes the record there as JSON).
 """
 import os
 import time
@@ -158,6 +159,7 @@ def test_time_reference_vs_ours(ref_mod):
            "ours_gbs": b / t_ours / 1e6, "speedup": t_ref / t_ours, "ref_csr_ms": t_csr,
            "speedup_vs_csr": (t_csr / t_ours) if t_csr else None, "when": time.time()}
     print("REFTIMING", json.dumps(rec))
-    os.makedirs("gpurun_out", exist_ok=True)
-    with open("gpurun_out/ref_timing.json", "w") as f:
-        json.dump(rec, f)
+    out = os.environ.get("CBM_REF_TIMING_OUT")
+    if out:
+        with open(out, "w") as f:
+            json.dump(rec, f)
