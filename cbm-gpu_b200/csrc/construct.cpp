@@ -101,45 +101,82 @@ inline int64_t floor_div2(int64_t x) { return x >= 0 ? x / 2 : -((-x + 1) / 2); 
 // contain a column of A[l]; candidates are activated there and their exact
 // overlap is completed over the remaining t - 1 columns, dropping those that
 // can no longer reach t.
+// Stable counting sort of 0..n-1 by key[i] (small non-negative integers): the
+// order std::stable_sort by key gives, in O(n + max key).
+template <typename K>
+std::vector<int32_t> order_by_key(const std::vector<K>& key) {
+  const int64_t n = (int64_t)key.size();
+  K kmax = 0;
+  for (int64_t i = 0; i < n; ++i) kmax = std::max(kmax, key[i]);
+  std::vector<int64_t> start((size_t)kmax + 2, 0);
+  for (int64_t i = 0; i < n; ++i) start[(size_t)key[i] + 1]++;
+  for (size_t b = 0; b + 1 < start.size(); ++b) start[b + 1] += start[b];
+  std::vector<int32_t> order(n);
+  for (int64_t i = 0; i < n; ++i) order[start[(size_t)key[i]]++] = (int32_t)i;
+  return order;
+}
+
 std::vector<Pair> candidate_pairs(const Csr& a, int64_t alpha, int n_threads) {
   const int64_t n = a.n;
-  std::vector<int32_t> rowlen(n);
-  for (int64_t i = 0; i < n; ++i) rowlen[i] = (int32_t)(a.ptr[i + 1] - a.ptr[i]);
-
-  // column counts and rarity rank
-  std::vector<int64_t> colcnt(n, 0);
-  for (int64_t k = 0; k < (int64_t)a.idx.size(); ++k) colcnt[a.idx[k]]++;
-  std::vector<int32_t> by_rarity(n);
-  std::iota(by_rarity.begin(), by_rarity.end(), 0);
-  std::stable_sort(by_rarity.begin(), by_rarity.end(),
-                   [&](int32_t x, int32_t y) { return colcnt[x] < colcnt[y]; });
-  std::vector<int32_t> rank(n);
-  for (int64_t r = 0; r < n; ++r) rank[by_rarity[r]] = (int32_t)r;
-
-  // rows ordered by (rowlen, id): position of each row in that order
-  std::vector<int32_t> by_size(n);
-  std::iota(by_size.begin(), by_size.end(), 0);
-  std::stable_sort(by_size.begin(), by_size.end(),
-                   [&](int32_t x, int32_t y) { return rowlen[x] < rowlen[y]; });
-  std::vector<int32_t> size_pos(n);
-  for (int64_t r = 0; r < n; ++r) size_pos[by_size[r]] = (int32_t)r;
-
-  // inverted lists: rows containing column c, ordered by size_pos
-  std::vector<int64_t> iptr(n + 1, 0);
-  for (int64_t c = 0; c < n; ++c) iptr[c + 1] = iptr[c] + colcnt[c];
-  std::vector<int32_t> inv(a.idx.size());
-  {
-    std::vector<int64_t> fill(iptr.begin(), iptr.end() - 1);
-    for (int64_t r = 0; r < n; ++r) {
-      int32_t row = by_size[r];
-      for (int64_t k = a.ptr[row]; k < a.ptr[row + 1]; ++k) inv[fill[a.idx[k]]++] = row;
-    }
-  }
-
   int nt = 1;
 #ifdef _OPENMP
   nt = n_threads > 0 ? n_threads : omp_get_max_threads();
 #endif
+  std::vector<int32_t> rowlen(n);
+  for (int64_t i = 0; i < n; ++i) rowlen[i] = (int32_t)(a.ptr[i + 1] - a.ptr[i]);
+
+  // column counts and rarity rank (column count, then id)
+  std::vector<int64_t> colcnt(n, 0);
+  for (int64_t k = 0; k < (int64_t)a.idx.size(); ++k) colcnt[a.idx[k]]++;
+  std::vector<int32_t> by_rarity = order_by_key(colcnt);
+  std::vector<int32_t> rank(n);
+  for (int64_t r = 0; r < n; ++r) rank[by_rarity[r]] = (int32_t)r;
+
+  // rows ordered by (rowlen, id): position of each row in that order
+  std::vector<int32_t> by_size = order_by_key(rowlen);
+  std::vector<int32_t> size_pos(n);
+  for (int64_t r = 0; r < n; ++r) size_pos[by_size[r]] = (int32_t)r;
+
+  // inverted lists: the size positions of the rows containing column c, in
+  // increasing order (positions, not row ids: the searches and scans below then
+  // compare plain integers; by_size maps a position back to its row).  Built in
+  // parallel: thread t fills the positions of its own contiguous range of
+  // positions after those of threads 0..t-1, so every list stays sorted.
+  std::vector<int64_t> iptr(n + 1, 0);
+  for (int64_t c = 0; c < n; ++c) iptr[c + 1] = iptr[c] + colcnt[c];
+  std::vector<int32_t> inv(a.idx.size());
+  {
+    const int parts = std::max(1, std::min<int>(nt, (int)std::max<int64_t>(1, n / 65536)));
+    std::vector<std::vector<int64_t>> fill(parts);
+#pragma omp parallel for num_threads(parts) schedule(static, 1)
+    for (int t = 0; t < parts; ++t) {
+      fill[t].assign(n, 0);
+      const int64_t r0 = n * t / parts, r1 = n * (t + 1) / parts;
+      for (int64_t r = r0; r < r1; ++r) {
+        const int32_t row = by_size[r];
+        for (int64_t k = a.ptr[row]; k < a.ptr[row + 1]; ++k) fill[t][a.idx[k]]++;
+      }
+    }
+    // per column: exclusive offsets of each part, starting at the column's list
+#pragma omp parallel for num_threads(nt) schedule(static)
+    for (int64_t c = 0; c < n; ++c) {
+      int64_t o = iptr[c];
+      for (int t = 0; t < parts; ++t) {
+        const int64_t k = fill[t][c];
+        fill[t][c] = o;
+        o += k;
+      }
+    }
+#pragma omp parallel for num_threads(parts) schedule(static, 1)
+    for (int t = 0; t < parts; ++t) {
+      const int64_t r0 = n * t / parts, r1 = n * (t + 1) / parts;
+      for (int64_t r = r0; r < r1; ++r) {
+        const int32_t row = by_size[r];
+        for (int64_t k = a.ptr[row]; k < a.ptr[row + 1]; ++k) inv[fill[t][a.idx[k]]++] = (int32_t)r;
+      }
+    }
+  }
+
   std::vector<std::vector<Pair>> out(nt);
 
 #pragma omp parallel num_threads(nt)
@@ -148,7 +185,12 @@ std::vector<Pair> candidate_pairs(const Csr& a, int64_t alpha, int n_threads) {
 #ifdef _OPENMP
     tid = omp_get_thread_num();
 #endif
-    std::vector<int32_t> stamp(n, -1), cnt(n, 0);
+    // indexed by size position; stamp and count side by side (one cache line
+    // per candidate touched)
+    struct Slot {
+      int32_t stamp, cnt;
+    };
+    std::vector<Slot> slot(n, Slot{-1, 0});
     std::vector<int32_t> cand, cols;
     std::vector<Pair>& mine = out[tid];
 
@@ -164,22 +206,19 @@ std::vector<Pair> candidate_pairs(const Csr& a, int64_t alpha, int n_threads) {
       std::sort(cols.begin(), cols.end(), [&](int32_t x, int32_t y) { return rank[x] < rank[y]; });
       const int32_t my_pos = size_pos[s];
       cand.clear();
-      // prefix: activate
+      // prefix: activate (candidates are the larger rows: positions above my_pos)
       for (int64_t j = 0; j < plen; ++j) {
         const int32_t c = cols[j];
         const int32_t* lb = inv.data() + iptr[c];
         const int32_t* le = inv.data() + iptr[c + 1];
-        const int32_t* st = std::upper_bound(lb, le, my_pos, [&](int32_t pos, int32_t row) {
-          return pos < size_pos[row];
-        });
-        for (const int32_t* p = st; p < le; ++p) {
+        for (const int32_t* p = std::upper_bound(lb, le, my_pos); p < le; ++p) {
           const int32_t l = *p;
-          if (stamp[l] != s) {
-            stamp[l] = s;
-            cnt[l] = 1;
+          if (slot[l].stamp != s) {
+            slot[l].stamp = s;
+            slot[l].cnt = 1;
             cand.push_back(l);
           } else {
-            cnt[l]++;
+            slot[l].cnt++;
           }
         }
       }
@@ -190,39 +229,38 @@ std::vector<Pair> candidate_pairs(const Csr& a, int64_t alpha, int n_threads) {
         const int64_t remaining_after = ns - j - 1;
         const int32_t* lb = inv.data() + iptr[c];
         const int32_t* le = inv.data() + iptr[c + 1];
-        const int32_t* st = std::upper_bound(lb, le, my_pos, [&](int32_t pos, int32_t row) {
-          return pos < size_pos[row];
-        });
+        const int32_t* st = std::upper_bound(lb, le, my_pos);
         if ((le - st) <= live * 8) {
           for (const int32_t* p = st; p < le; ++p)
-            if (stamp[*p] == s) cnt[*p]++;
+            if (slot[*p].stamp == s) slot[*p].cnt++;
         } else {
           for (int64_t q = 0; q < live; ++q) {
-            const int32_t l = cand[q];
+            const int32_t l = by_size[cand[q]];
             const int32_t* rb = a.idx.data() + a.ptr[l];
             const int32_t* re = a.idx.data() + a.ptr[l + 1];
-            if (std::binary_search(rb, re, c)) cnt[l]++;
+            if (std::binary_search(rb, re, c)) slot[cand[q]].cnt++;
           }
         }
         // prune
         int64_t w = 0;
         for (int64_t q = 0; q < live; ++q) {
           const int32_t l = cand[q];
-          if (cnt[l] + remaining_after >= t) {
+          if (slot[l].cnt + remaining_after >= t) {
             cand[w++] = l;
           } else {
-            stamp[l] = -2;  // dead for this s (stamps are row ids >= 0)
+            slot[l].stamp = -2;  // dead for this s (stamps are row ids >= 0)
           }
         }
         live = w;
       }
       for (int64_t q = 0; q < live; ++q) {
-        const int32_t l = cand[q];
-        if (cnt[l] >= t) {
+        const int32_t lp = cand[q];
+        if (slot[lp].cnt >= t) {
+          const int32_t l = by_size[lp];
           Pair p;
           p.lo = std::min(s, l);
           p.hi = std::max(s, l);
-          p.o = cnt[l];
+          p.o = slot[lp].cnt;
           mine.push_back(p);
         }
       }
@@ -484,21 +522,62 @@ struct cbm_structure {
 
 namespace {
 
-void emit(cbm_structure& out, const Csr& a, const std::vector<std::vector<int32_t>>& children) {
+// Entries of A[v] - A[u] (u = -1: A[v] as +1 entries) in increasing column
+// order, written at out (when not null); returns their number.
+int64_t delta_block(const Csr& a, int32_t u, int32_t v, int32_t* row, int32_t* col, float* val) {
+  int64_t m = 0;
+  auto put = [&](int32_t c, float s) {
+    if (row) {
+      row[m] = v;
+      col[m] = c;
+      val[m] = s;
+    }
+    ++m;
+  };
+  int64_t vp = a.ptr[v], ve = a.ptr[v + 1];
+  if (u < 0) {
+    for (; vp < ve; ++vp) put(a.idx[vp], 1.0f);
+    return m;
+  }
+  int64_t up = a.ptr[u], ue = a.ptr[u + 1];
+  while (up < ue && vp < ve) {
+    const int32_t cu = a.idx[up], cv = a.idx[vp];
+    if (cu == cv) {
+      ++up;
+      ++vp;
+    } else if (cu > cv) {
+      put(cv, 1.0f);
+      ++vp;
+    } else {
+      put(cu, -1.0f);
+      ++up;
+    }
+  }
+  for (; up < ue; ++up) put(a.idx[up], -1.0f);
+  for (; vp < ve; ++vp) put(a.idx[vp], 1.0f);
+  return m;
+}
+
+// Delta entries and tree edges in the reference's order
+// (cbm/cbm_extensions.cpp:220-294): first the root children's whole rows as
+// +1 entries, then for each non-empty branch, in BFS order, every tree edge
+// (u, v) and the entries of A[v] - A[u] by a sorted merge.  The block of each
+// emitted row is sized first, then all blocks are written in parallel at
+// their offsets, so the output equals the sequential emission.
+void emit(cbm_structure& out, const Csr& a, const std::vector<std::vector<int32_t>>& children, int n_threads) {
   const int64_t n = a.n;
   const auto& roots = children[n];
   std::vector<int32_t> non_empty;
   for (int32_t v : roots)
     if (!children[v].empty()) non_empty.push_back(v);
-  // root children: their whole row as +1 (cbm/cbm_extensions.cpp:220-230)
+  // blocks in output order: (u, v) with u = -1 for root children
+  std::vector<int32_t> bu, bv;
+  bu.reserve(n);
+  bv.reserve(n);
   for (int32_t v : roots) {
-    for (int64_t k = a.ptr[v]; k < a.ptr[v + 1]; ++k) {
-      out.delta_row.push_back(v);
-      out.delta_col.push_back(a.idx[k]);
-      out.delta_val.push_back(1.0f);
-    }
+    bu.push_back(-1);
+    bv.push_back(v);
   }
-  // BFS over non-empty branches (cbm/cbm_extensions.cpp:232-294)
   out.branches.assign(non_empty.size() + 1, 0);
   std::deque<int32_t> fifo;
   for (size_t b = 0; b < non_empty.size(); ++b) {
@@ -511,38 +590,28 @@ void emit(cbm_structure& out, const Csr& a, const std::vector<std::vector<int32_
         out.src.push_back(u);
         out.dst.push_back(v);
         out.branches[b + 1]++;
-        int64_t up = a.ptr[u], ue = a.ptr[u + 1], vp = a.ptr[v], ve = a.ptr[v + 1];
-        while (up < ue && vp < ve) {
-          const int32_t cu = a.idx[up], cv = a.idx[vp];
-          if (cu == cv) {
-            ++up;
-            ++vp;
-          } else if (cu > cv) {
-            out.delta_row.push_back(v);
-            out.delta_col.push_back(cv);
-            out.delta_val.push_back(1.0f);
-            ++vp;
-          } else {
-            out.delta_row.push_back(v);
-            out.delta_col.push_back(cu);
-            out.delta_val.push_back(-1.0f);
-            ++up;
-          }
-        }
-        for (; up < ue; ++up) {
-          out.delta_row.push_back(v);
-          out.delta_col.push_back(a.idx[up]);
-          out.delta_val.push_back(-1.0f);
-        }
-        for (; vp < ve; ++vp) {
-          out.delta_row.push_back(v);
-          out.delta_col.push_back(a.idx[vp]);
-          out.delta_val.push_back(1.0f);
-        }
+        bu.push_back(u);
+        bv.push_back(v);
       }
     }
   }
   std::partial_sum(out.branches.begin(), out.branches.end(), out.branches.begin());
+  const int64_t nb = (int64_t)bu.size();
+  std::vector<int64_t> off(nb + 1, 0);
+  int nt = 1;
+#ifdef _OPENMP
+  nt = n_threads > 0 ? n_threads : omp_get_max_threads();
+#endif
+#pragma omp parallel for num_threads(nt) schedule(dynamic, 1024)
+  for (int64_t k = 0; k < nb; ++k) off[k + 1] = delta_block(a, bu[k], bv[k], nullptr, nullptr, nullptr);
+  for (int64_t k = 0; k < nb; ++k) off[k + 1] += off[k];
+  out.delta_row.resize(off[nb]);
+  out.delta_col.resize(off[nb]);
+  out.delta_val.resize(off[nb]);
+#pragma omp parallel for num_threads(nt) schedule(dynamic, 1024)
+  for (int64_t k = 0; k < nb; ++k)
+    delta_block(a, bu[k], bv[k], out.delta_row.data() + off[k], out.delta_col.data() + off[k],
+                out.delta_val.data() + off[k]);
 }
 
 }  // namespace
@@ -620,20 +689,29 @@ int cbm_build_clustered(const int32_t* row, const int32_t* col, int64_t nnz, int
       children[g.from[e]].push_back(g.to[e]);
       s->parent[g.to[e]] = g.from[e];
     }
-    emit(*s, a, children);
+    emit(*s, a, children, n_threads);
     // Each node's delta entries are emitted as one block in increasing column
     // order, so the CSR form is a permutation of those blocks.
+    // A block starts where the row id changes, so each row's first entry and
+    // length are found in parallel, each row written by one k.
     const int64_t z = (int64_t)s->delta_row.size();
+    const int32_t* dr = s->delta_row.data();
+    int nt = 1;
+#ifdef _OPENMP
+    nt = n_threads > 0 ? n_threads : omp_get_max_threads();
+#endif
     s->csr_ptr.assign(n + 1, 0);
     std::vector<int64_t> first(n, -1);
-    for (int64_t k = 0; k < z; ++k) {
-      const int32_t r = s->delta_row[k];
-      if (first[r] < 0) first[r] = k;
-      s->csr_ptr[r + 1]++;
-    }
+#pragma omp parallel for num_threads(nt) schedule(static)
+    for (int64_t k = 0; k < z; ++k)
+      if (k == 0 || dr[k - 1] != dr[k]) first[dr[k]] = k;
+#pragma omp parallel for num_threads(nt) schedule(static)
+    for (int64_t k = 0; k < z; ++k)
+      if (k == z - 1 || dr[k + 1] != dr[k]) s->csr_ptr[dr[k] + 1] = (int32_t)(k + 1 - first[dr[k]]);
     for (int64_t i = 0; i < n; ++i) s->csr_ptr[i + 1] += s->csr_ptr[i];
     s->csr_col.resize(z);
     s->csr_val.resize(z);
+#pragma omp parallel for num_threads(nt) schedule(dynamic, 4096)
     for (int64_t i = 0; i < n; ++i) {
       const int64_t len = s->csr_ptr[i + 1] - s->csr_ptr[i];
       if (len == 0) continue;
