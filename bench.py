@@ -362,8 +362,9 @@ def run_precision(args):
     else:
         from cbm.tune import autotune
 
-        tuned = autotune(a.plan, "adx", x, y, space={"chunk_nnz": [256, 512], "rows_per_claim": [2, 4, 8],
-                                                     "variant": ["auto", "register", "tma"]})
+        tuned = autotune(a.plan, "adx", x, y, space={"chunk_nnz": [256, 512], "rows_per_claim": [4, 8, 16],
+                                                     "variant": ["auto", "register", "tma"],
+                                                     "hot_rows": [65536, 262144]})
     ms = _time_events(lambda: a.matmul(x, y), args.steps, args.warmup)
     dinv = dinv_f64(ei, n)
     err = {"product": fp64_sample_error(ei, n, x, y, cs=dinv),
