@@ -59,6 +59,20 @@ Csr coo_to_csr(const int32_t* row, const int32_t* col, int64_t nnz, int64_t n) {
   Csr a;
   a.n = n;
   a.ptr.assign(n + 1, 0);
+  // already coalesced (sorted by row, then strictly by column): the CSR is the
+  // column array itself, the row pointers are where the row id changes
+  bool coalesced = true;
+#pragma omp parallel for reduction(&& : coalesced) schedule(static)
+  for (int64_t k = 1; k < nnz; ++k)
+    if (row[k] < row[k - 1] || (row[k] == row[k - 1] && col[k] <= col[k - 1])) coalesced = false;
+  if (coalesced) {
+#pragma omp parallel for schedule(static)
+    for (int64_t k = 0; k < nnz; ++k)
+      if (k == nnz - 1 || row[k + 1] != row[k]) a.ptr[row[k] + 1] = k + 1;
+    for (int64_t i = 0; i < n; ++i) a.ptr[i + 1] = std::max(a.ptr[i + 1], a.ptr[i]);
+    a.idx.assign(col, col + nnz);
+    return a;
+  }
   for (int64_t k = 0; k < nnz; ++k) a.ptr[row[k] + 1]++;
   for (int64_t i = 0; i < n; ++i) a.ptr[i + 1] += a.ptr[i];
   std::vector<int32_t> tmp(nnz);

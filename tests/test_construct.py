@@ -209,3 +209,19 @@ def test_structure_cache_round_trip(tmp_path):
     np.testing.assert_array_equal(s3.csr_col, cbm_mkl_cpp.build(ei[0], ei[1], 700, 0).csr_col)
     # a file of another format or key is ignored
     assert cbm_mkl_cpp.load_structure(str(files[0]), key="other") is None
+
+
+def test_coalesced_and_shuffled_inputs_give_the_same_structure():
+    """Coalesced COO takes the constructor's direct CSR path; the same edges
+    shuffled (and with duplicates) take the sorting path: same structure."""
+    from cbm import cbm_mkl_cpp
+    from conftest import near_dup_graph
+
+    ei = near_dup_graph(900, seed=14)
+    s0 = cbm_mkl_cpp.build(ei[0], ei[1], 900, 3)
+    perm = np.random.default_rng(0).permutation(ei.shape[1])
+    dup = np.concatenate([perm, perm[:200]])
+    s1 = cbm_mkl_cpp.build(np.ascontiguousarray(ei[0][dup]), np.ascontiguousarray(ei[1][dup]), 900, 3)
+    for f in ("csr_ptr", "csr_col", "csr_val", "branches", "src", "dst", "parent"):
+        np.testing.assert_array_equal(getattr(s0, f), getattr(s1, f))
+    assert s0.nnz_a == s1.nnz_a == ei.shape[1]
