@@ -638,7 +638,9 @@ int matmul_impl(cbm_plan* P, int32_t op, float gin_scale, const void* x, int32_t
     // 40 FP32 columns, 0.35 -> 0.23 ms at 128 BF16 columns; the 1M-node and
     // 2.4M-node power-law graphs, 5 % and 40 % below level 0, keep the staged
     // kernel).
-    const bool deep_tree = (P->n_items - P->n_root) * 2 > P->n_items;
+    // (rows of at most 512 bytes: the widths measured; wider rows keep the
+    // staged kernel, whose ring carries more bytes in flight per lane)
+    const bool deep_tree = (P->n_items - P->n_root) * 2 > P->n_items && cols * elem_size(xdt) <= 512;
     const bool staged = sh.vec && !gin && P->variant != CBM_VARIANT_REGISTER &&
                         !(P->variant == CBM_VARIANT_AUTO && deep_tree) &&
                         staged_shape(nvec, sh.v, P->staged_team, &s_team, &s_vpl);

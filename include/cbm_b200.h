@@ -160,7 +160,8 @@ int cbm_plan_set_multipliers(cbm_plan* plan, const float* d_multipliers, void* s
  * Changing chunk_nnz or hot_rows re-lays out the plan (synchronous). */
 enum {
   CBM_VARIANT_AUTO = 0,     /* staged where it applies, else register gather; register
-                               gather also when most rows hang below tree level 0 */
+                               gather also for rows of at most 512 bytes when most rows
+                               hang below tree level 0 */
   CBM_VARIANT_REGISTER = 1, /* X rows gathered into registers, U entries at a time */
   CBM_VARIANT_STAGED = 2,   /* X rows staged through shared memory by cp.async */
   CBM_VARIANT_TMA = 3       /* X rows gathered four at a time by TMA (tile::gather4) into
