@@ -1,0 +1,13 @@
+// Register-gather forward kernel instantiations, BF16 X.
+#include "launch.cuh"
+
+namespace cbm {
+int launch_fwd_bf16(cbm_plan* P, const FwdArgs& a, int32_t ydt, bool vec, int vpl, cudaStream_t st) {
+  if (ydt == CBM_F32) {
+    return vec ? launch_fwd_v<__nv_bfloat16, float, 8>(P, a, vpl, st)
+               : launch_fwd_v<__nv_bfloat16, float, 1>(P, a, vpl, st);
+  }
+  return vec ? launch_fwd_v<__nv_bfloat16, __nv_bfloat16, 8>(P, a, vpl, st)
+             : launch_fwd_v<__nv_bfloat16, __nv_bfloat16, 1>(P, a, vpl, st);
+}
+}  // namespace cbm

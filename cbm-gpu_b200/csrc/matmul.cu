@@ -1,33 +1,29 @@
-// Launch side of the CBM product: operand checks, tile-shape selection and the
-// kernel instantiations behind cbm_matmul / cbm_matmul_adjoint.
+// Launch side of the CBM product: operand checks, tile-shape selection, the
+// adjoint layout and the host-operand pipeline behind cbm_matmul /
+// cbm_matmul_adjoint / cbm_matmul_host.  The kernel instantiations live in the
+// launch_*.cu units (launch.cuh).
 
 #include "cbm_b200.h"
-#include "kernels.cuh"
-#include "plan.h"
+#include "launch.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <vector>
 
 namespace cbm {
-namespace {
 
 int sm_count(int device) {
-  static int cached_dev = -1, cached = 0;
-  if (cached_dev != device) {
-    cudaDeviceGetAttribute(&cached, cudaDevAttrMultiProcessorCount, device);
-    cached_dev = device;
-  }
-  return cached > 0 ? cached : 1;
+  static std::atomic<int> count[kMaxDevices];
+  if (device < 0 || device >= kMaxDevices) return 1;
+  int c = count[device].load(std::memory_order_acquire);
+  if (c > 0) return c;
+  if (cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || c < 1) return 1;
+  count[device].store(c, std::memory_order_release);
+  return c;
 }
 
-template <typename K>
-int grid_for(K kernel, int device) {
-  int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, 0) != cudaSuccess || per_sm < 1)
-    per_sm = 1;
-  return per_sm * sm_count(device);
-}
+namespace {
 
 int64_t round4(int64_t x) { return (x + 3) / 4 * 4; }
 
@@ -86,47 +82,6 @@ int64_t extent(int64_t rows, int64_t ld, int64_t cols, int32_t dt) {
 bool overlaps(const void* a, int64_t abytes, const void* b, int64_t bbytes) {
   const uintptr_t a0 = reinterpret_cast<uintptr_t>(a), b0 = reinterpret_cast<uintptr_t>(b);
   return a0 < b0 + (uintptr_t)bbytes && b0 < a0 + (uintptr_t)abytes;
-}
-
-// ---- forward launch ------------------------------------------------------------
-template <typename XT, typename YT, int VPL, int V, bool COMP = false>
-int launch_fwd_t(cbm_plan* P, const FwdArgs& a, cudaStream_t st) {
-  static int grid_cache = 0, grid_dev = -1;
-  if (grid_dev != P->device) {
-    grid_cache = grid_for(fwd_kernel<XT, YT, VPL, V, COMP>, P->device);
-    grid_dev = P->device;
-  }
-  fwd_kernel<XT, YT, VPL, V, COMP><<<grid_cache, kThreads, 0, st>>>(a);
-  P->launches++;
-  P->last_grid = grid_cache;
-  return cuda_status(cudaGetLastError());
-}
-
-// Staged kernel: ring of S slots of VPL 16-byte pieces per thread, blocks of
-// 128 threads.
-constexpr int kStagedBlock = 128;
-
-template <typename XT, typename YT, int TL, int VPL, int V, int S, bool TMA = false>
-int launch_stream_t(cbm_plan* P, const FwdArgs& a, const CUtensorMap& map, cudaStream_t st) {
-  static int grid_cache = 0, grid_dev = -1, grid_smem = -1;
-  constexpr int n_teams = kStagedBlock / TL;
-  const int smem = TMA ? n_teams * (S / 4) * (4 * a.tma_rb + 8) : S * VPL * kStagedBlock * 16;
-  auto kern = fwd_stream_kernel<XT, YT, TL, VPL, V, S, kStagedBlock, TMA>;
-  if (grid_dev != P->device || grid_smem != smem) {
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
-      return CBM_ERR_CUDA;
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kStagedBlock, smem) != cudaSuccess ||
-        per_sm < 1)
-      per_sm = 1;
-    grid_cache = per_sm * sm_count(P->device);
-    grid_dev = P->device;
-    grid_smem = smem;
-  }
-  kern<<<grid_cache, kStagedBlock, smem, st>>>(a, map);
-  P->launches++;
-  P->last_grid = grid_cache;
-  return cuda_status(cudaGetLastError());
 }
 
 // cuTensorMapEncodeTiled from the driver, found once through the runtime
@@ -189,54 +144,10 @@ bool staged_shape(int64_t nvec, int v, int forced, int* team, int* vpl) {
   return true;
 }
 
-template <typename XT, typename YT, int TL>
-int launch_staged_team(cbm_plan* P, const FwdArgs& a, int vpl, const CUtensorMap& map, cudaStream_t st) {
-  constexpr int V = 16 / (int)sizeof(XT);
-  // one piece per lane: a deeper ring (16 slots, 32 KiB per block) keeps as
-  // many bytes in flight as two pieces in 8 slots
-  constexpr int S1 = TL >= 16 ? 16 : 8;
-  switch (vpl) {
-    case 1: return launch_stream_t<XT, YT, TL, 1, V, S1>(P, a, map, st);
-    case 2: return launch_stream_t<XT, YT, TL, 2, V, 8>(P, a, map, st);
-    case 4: return launch_stream_t<XT, YT, TL, 4, V, 8>(P, a, map, st);
-    default:
-      if constexpr (V == 4) return launch_stream_t<XT, YT, TL, 8, V, 4>(P, a, map, st);
-      return CBM_ERR_INTERNAL;
-  }
-}
-
-template <typename XT, typename YT>
-int launch_staged_any(cbm_plan* P, const FwdArgs& a, int team, int vpl, const CUtensorMap& map, cudaStream_t st) {
-  if (team == 8) return launch_staged_team<XT, YT, 8>(P, a, vpl, map, st);
-  if (team == 16) return launch_staged_team<XT, YT, 16>(P, a, vpl, map, st);
-  return launch_staged_team<XT, YT, 32>(P, a, vpl, map, st);
-}
-
 int launch_staged(cbm_plan* P, const FwdArgs& a, int32_t xdt, int32_t ydt, int team, int vpl, cudaStream_t st) {
-  CUtensorMap none;
-  std::memset(&none, 0, sizeof(none));
-  if (xdt == CBM_F32) return launch_staged_any<float, float>(P, a, team, vpl, none, st);
-  if (ydt == CBM_F32) return launch_staged_any<__nv_bfloat16, float>(P, a, team, vpl, none, st);
-  return launch_staged_any<__nv_bfloat16, __nv_bfloat16>(P, a, team, vpl, none, st);
-}
-
-// TMA variant: every lane owns every piece (nvec == team * vpl), one or two
-// pieces per lane; ring depths as in the cp.async variant.
-template <typename XT, typename YT>
-int launch_tma_any(cbm_plan* P, const FwdArgs& a, int team, int vpl, const CUtensorMap& map, cudaStream_t st) {
-  constexpr int V = 16 / (int)sizeof(XT);
-  if (team == 8 && vpl == 1) return launch_stream_t<XT, YT, 8, 1, V, 8, true>(P, a, map, st);
-  if (team == 16 && vpl == 1) return launch_stream_t<XT, YT, 16, 1, V, 16, true>(P, a, map, st);
-  if (team == 32 && vpl == 1) return launch_stream_t<XT, YT, 32, 1, V, 16, true>(P, a, map, st);
-  if (team == 32 && vpl == 2) return launch_stream_t<XT, YT, 32, 2, V, 8, true>(P, a, map, st);
-  return CBM_ERR_INTERNAL;
-}
-
-int launch_tma(cbm_plan* P, const FwdArgs& a, int32_t xdt, int32_t ydt, int team, int vpl, const CUtensorMap& map,
-               cudaStream_t st) {
-  if (xdt == CBM_F32) return launch_tma_any<float, float>(P, a, team, vpl, map, st);
-  if (ydt == CBM_F32) return launch_tma_any<__nv_bfloat16, float>(P, a, team, vpl, map, st);
-  return launch_tma_any<__nv_bfloat16, __nv_bfloat16>(P, a, team, vpl, map, st);
+  if (xdt == CBM_F32) return launch_staged_f32(P, a, team, vpl, st);
+  if (ydt == CBM_F32) return launch_staged_bf16_f32(P, a, team, vpl, st);
+  return launch_staged_bf16_bf16(P, a, team, vpl, st);
 }
 
 // The TMA variant applies to 16-byte-vector rows of a power-of-two number of
@@ -246,93 +157,9 @@ bool tma_shape(int64_t nvec, int v, int team, int vpl) {
   return nvec >= 8 && (nvec & (nvec - 1)) == 0 && nvec == (int64_t)team * vpl && nvec * v <= 256 && vpl <= 2;
 }
 
-template <typename XT, typename YT, int V, bool COMP = false>
-int launch_fwd_v(cbm_plan* P, const FwdArgs& a, int vpl, cudaStream_t st) {
-  switch (vpl) {
-    case 1: return launch_fwd_t<XT, YT, 1, V, COMP>(P, a, st);
-    case 2: return launch_fwd_t<XT, YT, 2, V, COMP>(P, a, st);
-    case 4: return launch_fwd_t<XT, YT, 4, V, COMP>(P, a, st);
-    default: return launch_fwd_t<XT, YT, 8, V, COMP>(P, a, st);
-  }
-}
-
-// compensated propagation: BF16 X only (the precision form), register kernel
-int launch_fwd_comp(cbm_plan* P, const FwdArgs& a, int32_t ydt, bool vec, int vpl, cudaStream_t st) {
-  if (ydt == CBM_F32) {
-    return vec ? launch_fwd_v<__nv_bfloat16, float, 8, true>(P, a, vpl, st)
-               : launch_fwd_v<__nv_bfloat16, float, 1, true>(P, a, vpl, st);
-  }
-  return vec ? launch_fwd_v<__nv_bfloat16, __nv_bfloat16, 8, true>(P, a, vpl, st)
-             : launch_fwd_v<__nv_bfloat16, __nv_bfloat16, 1, true>(P, a, vpl, st);
-}
-
 int launch_fwd(cbm_plan* P, const FwdArgs& a, int32_t xdt, int32_t ydt, bool vec, int vpl, cudaStream_t st) {
-  if (xdt == CBM_F32) {
-    return vec ? launch_fwd_v<float, float, 4>(P, a, vpl, st) : launch_fwd_v<float, float, 1>(P, a, vpl, st);
-  }
-  if (ydt == CBM_F32) {
-    return vec ? launch_fwd_v<__nv_bfloat16, float, 8>(P, a, vpl, st)
-               : launch_fwd_v<__nv_bfloat16, float, 1>(P, a, vpl, st);
-  }
-  return vec ? launch_fwd_v<__nv_bfloat16, __nv_bfloat16, 8>(P, a, vpl, st)
-             : launch_fwd_v<__nv_bfloat16, __nv_bfloat16, 1>(P, a, vpl, st);
-}
-
-// ---- adjoint launches -------------------------------------------------------------
-template <typename GT, int VPL, int V>
-int launch_rev_t(cbm_plan* P, const RevArgs& a, cudaStream_t st) {
-  static int grid_cache = 0, grid_dev = -1;
-  if (grid_dev != P->device) {
-    grid_cache = grid_for(rev_kernel<GT, VPL, V>, P->device);
-    grid_dev = P->device;
-  }
-  rev_kernel<GT, VPL, V><<<grid_cache, kThreads, 0, st>>>(a);
-  P->launches++;
-  return cuda_status(cudaGetLastError());
-}
-template <typename GT, typename DT, int VPL, int V>
-int launch_tr_t(cbm_plan* P, const TrArgs& a, cudaStream_t st) {
-  static int grid_cache = 0, grid_dev = -1;
-  if (grid_dev != P->device) {
-    grid_cache = grid_for(tr_kernel<GT, DT, VPL, V>, P->device);
-    grid_dev = P->device;
-  }
-  tr_kernel<GT, DT, VPL, V><<<grid_cache, kThreads, 0, st>>>(a);
-  P->launches++;
-  return cuda_status(cudaGetLastError());
-}
-template <typename GT, int V>
-int launch_rev_v(cbm_plan* P, const RevArgs& a, int vpl, cudaStream_t st) {
-  switch (vpl) {
-    case 1: return launch_rev_t<GT, 1, V>(P, a, st);
-    case 2: return launch_rev_t<GT, 2, V>(P, a, st);
-    case 4: return launch_rev_t<GT, 4, V>(P, a, st);
-    default: return launch_rev_t<GT, 8, V>(P, a, st);
-  }
-}
-template <typename GT, typename DT, int V>
-int launch_tr_v(cbm_plan* P, const TrArgs& a, int vpl, cudaStream_t st) {
-  switch (vpl) {
-    case 1: return launch_tr_t<GT, DT, 1, V>(P, a, st);
-    case 2: return launch_tr_t<GT, DT, 2, V>(P, a, st);
-    case 4: return launch_tr_t<GT, DT, 4, V>(P, a, st);
-    default: return launch_tr_t<GT, DT, 8, V>(P, a, st);
-  }
-}
-int launch_rev(cbm_plan* P, const RevArgs& a, int32_t gdt, bool vec, int vpl, cudaStream_t st) {
-  if (gdt == CBM_F32) return vec ? launch_rev_v<float, 4>(P, a, vpl, st) : launch_rev_v<float, 1>(P, a, vpl, st);
-  return vec ? launch_rev_v<__nv_bfloat16, 8>(P, a, vpl, st) : launch_rev_v<__nv_bfloat16, 1>(P, a, vpl, st);
-}
-int launch_tr(cbm_plan* P, const TrArgs& a, int32_t gdt, int32_t ddt, bool vec, int vpl, cudaStream_t st) {
-  if (gdt == CBM_F32) {
-    return vec ? launch_tr_v<float, float, 4>(P, a, vpl, st) : launch_tr_v<float, float, 1>(P, a, vpl, st);
-  }
-  if (ddt == CBM_F32) {
-    return vec ? launch_tr_v<__nv_bfloat16, float, 8>(P, a, vpl, st)
-               : launch_tr_v<__nv_bfloat16, float, 1>(P, a, vpl, st);
-  }
-  return vec ? launch_tr_v<__nv_bfloat16, __nv_bfloat16, 8>(P, a, vpl, st)
-             : launch_tr_v<__nv_bfloat16, __nv_bfloat16, 1>(P, a, vpl, st);
+  if (xdt == CBM_F32) return launch_fwd_f32(P, a, vec, vpl, st);
+  return launch_fwd_bf16(P, a, ydt, vec, vpl, st);
 }
 
 template <typename T>
