@@ -2,7 +2,8 @@
 
     python -m cbm._build            (from cbm-gpu_b200/)
 
-Sources: cbm-gpu_b200/csrc/{construct.cpp, plan.cu, matmul.cu, noalloc.cu, transpose.cu}; header include/.
+Sources: cbm-gpu_b200/csrc/*.cpp, *.cu (kernel instantiations split over the launch_*.cu units so
+they compile in parallel); header include/.
 Objects go to cbm-gpu_b200/_build/, the library next to this file.
 """
 from __future__ import annotations
@@ -22,8 +23,10 @@ BUILD = os.path.join(PKG_ROOT, "_build")
 LIB = os.path.join(HERE, "libcbm_b200.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["construct.cpp", "plan.cu", "matmul.cu", "noalloc.cu", "transpose.cu"]
-HEADERS = ["kernels.cuh", "plan.h"]
+SOURCES = ["construct.cpp", "plan.cu", "matmul.cu", "noalloc.cu", "transpose.cu", "launch_staged_f32.cu",
+           "launch_staged_bf16_f32.cu", "launch_staged_bf16_bf16.cu", "launch_tma.cu", "launch_reg_f32.cu",
+           "launch_reg_bf16.cu", "launch_rev.cu", "launch_tr.cu", "direct.cu"]
+HEADERS = ["kernels.cuh", "plan.h", "launch.cuh"]
 
 
 def _nvcc():
@@ -67,7 +70,7 @@ def build(verbose=False, force=False):
             raise RuntimeError("build failed:\n" + " ".join(cmd) + "\n" + r.stdout + r.stderr)
         return r
 
-    with ThreadPoolExecutor(max_workers=max(1, len(jobs))) as ex:
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 8))) as ex:
         list(ex.map(run, jobs))
     if jobs or force or _newer(LIB, objs):
         run([nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-Xcompiler", "-fopenmp", "-lgomp"])

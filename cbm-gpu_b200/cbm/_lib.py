@@ -57,6 +57,19 @@ SIGNATURES = [
     ("cbm_plan_debug_check_transpose", C.c_int, [vp, vp]),
     ("cbm_plan_error", C.c_int, [vp, vp, C.POINTER(i32), C.POINTER(i64)]),
     ("cbm_matmul_noalloc", C.c_int, [vp, vp, vp, i64, i64, vp, vp, i64, vp, vp, vp, i64, vp, vp]),
+    ("cbm_direct_workspace_bytes", i64, [i64]),
+    ("cbm_direct_status", C.c_int, [vp, vp, C.POINTER(i32), C.POINTER(i64)]),
+    ("cbm_s_spmm_csr_int32", C.c_int, [vp, vp, vp, vp, i64, i64, i64, vp, i64, vp, vp, i64, vp]),
+    ("cbm_s_spmm_csr_t_int32", C.c_int, [vp, vp, vp, vp, i64, i64, i64, vp, i64, vp, vp, i64, vp]),
+    ("cbm_s_spmm_add_csr_int32", C.c_int, [vp, vp, vp, vp, i64, i64, i64, vp, i64, C.c_float, vp, vp, i64, vp]),
+    ("cbm_s_spmm_update_csr_int32", C.c_int, [vp, vp, vp, vp, i64, i64, i64, vp, i64, vp, i64, vp, vp, i64, vp,
+                                              vp, i64, vp]),
+    ("cbm_s_spmm_fused_update_csr_int32", C.c_int, [vp, vp, vp, vp, i64, i64, i64, vp, i64, vp, i64, vp, vp, i64,
+                                                    vp, vp, vp, i64, vp]),
+    ("cbm_s_spmm_update_add_csr_int32", C.c_int, [vp, vp, vp, vp, i64, i64, i64, vp, i64, C.c_float, vp, i64, vp,
+                                                  vp, i64, vp, vp, i64, vp]),
+    ("cbm_s_update_csr_int32", C.c_int, [vp, i64, vp, vp, i64, vp, i64, i64, vp, i64, vp]),
+    ("cbm_s_fused_update_csr_int32", C.c_int, [vp, i64, vp, vp, i64, vp, vp, i64, i64, vp, i64, vp]),
     ("cbm_plan_stat", i64, [vp, i32]),
     ("cbm_plan_destroy", None, [vp]),
     ("cbm_status_string", C.c_char_p, [i32]),

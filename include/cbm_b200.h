@@ -25,6 +25,8 @@
  *                                     applied on the fly instead of pre-scaled values
  *                                     (cbm/cbm4ad.py:19-25, cbm/cbm4dad.py:19-34)
  *   cbm_matmul_adjoint                no counterpart: A^T*G in CBM form (autograd)
+ *   cbm_s_*_csr_int32                 the cbm_mkl_cpp operators    cbm/cbm_extensions.cpp:351-919
+ *                                     (stateless, on the reference's layout; one line each below)
  */
 #ifndef CBM_B200_H
 #define CBM_B200_H
@@ -277,6 +279,97 @@ int cbm_matmul_noalloc(const int32_t* row_ptr, const int32_t* col_idx, const flo
                        int64_t n_cols, const int32_t* src, const int32_t* dst, int64_t n_edges,
                        const float* multipliers, const float* x, float* y, int64_t n_x_cols, int32_t* d_status,
                        void* stream);
+
+/* ---- the reference's CPU operators on the GPU --------------------------------
+ * Stateless GPU counterparts of the eight products the reference's cbm_mkl_cpp
+ * module binds (cbm/cbm_extensions.cpp:909-919), on the reference's own
+ * layout: no plan, every call reads the caller's arrays.
+ *   A [n_rows, n_cols]: MKL's four-array CSR as the reference passes it --
+ *     rp_b / rp_e begin and end row pointers (crow[:-1], crow[1:]), col, val
+ *     (val NULL: every entry 1); entries lie in [0, nnz).
+ *   Tree: branch offsets (n_branch_offsets = branches + 1, a prefix sum from 0
+ *     to n_edges) and the (parent src, child dst) edges in BFS order per
+ *     branch: cbm_init_'s output (CBM_S_BRANCHES / CBM_S_SRC / CBM_S_DST).
+ *     Edges are processed in their listed order, parents before children.
+ *   rhs, out: contiguous row-major FP32 with n_rhs_cols columns.
+ * All pointers are device addresses.  workspace: device memory of at least
+ * cbm_direct_workspace_bytes(rows of out) bytes, 16-byte aligned, zero-filled
+ * once before its first use and then kept (a status word, a claim counter and
+ * two per-node stamps compared against a per-call value: never cleared again).
+ * Calls that share a workspace must be ordered (one stream).  Each call
+ * launches on `stream` without synchronising; index errors found on the device
+ * (CBM_ERR_INDEX), a node with two parents or bad branch offsets
+ * (CBM_ERR_STRUCTURE) and bounded waits that ran out (CBM_ERR_TIMEOUT: a child
+ * edge listed before its parent's) are recorded in the workspace and read with
+ * cbm_direct_status.
+ * Rounding: each row sums its entries in order, one FMA per entry (MKL's order
+ * may differ in the last bits); the update adds Y[v] + Y[u]; the fused update
+ * adds fma(Y[u], m[v] / m[u], Y[v]) (the reference's CPU rounding,
+ * cbm/cbm_extensions.cpp:660-697, not the GPU path's (Y[u] m[v]) / m[u]); the
+ * GIN term is fma(1 + epsilon, X, Y) (its cblas_saxpy).  The transposed
+ * product adds with atomics: its summation order is not deterministic. */
+int64_t cbm_direct_workspace_bytes(int64_t n_rows);
+
+/* Synchronises `stream`, returns the first device-side error the calls on this
+ * workspace recorded (CBM_OK if none) and clears it; info (may be NULL)
+ * receives the entry, row, edge or branch offset where it happened. */
+int cbm_direct_status(void* workspace, void* stream, int32_t* device_status, int64_t* info);
+
+/* out = A rhs.  Replaces s_spmm_csr_int32 (cbm/cbm_extensions.cpp:700-740). */
+int cbm_s_spmm_csr_int32(const int32_t* rp_b, const int32_t* rp_e, const int32_t* col, const float* val,
+                         int64_t n_rows, int64_t n_cols, int64_t nnz, const float* rhs, int64_t n_rhs_cols,
+                         float* out, void* workspace, int64_t workspace_bytes, void* stream);
+
+/* out [n_cols, C] = A^T rhs (rhs [n_rows, C]).  Replaces s_spmm_csr_t_int32
+ * (cbm/cbm_extensions.cpp:742-782), which declares A square. */
+int cbm_s_spmm_csr_t_int32(const int32_t* rp_b, const int32_t* rp_e, const int32_t* col, const float* val,
+                           int64_t n_rows, int64_t n_cols, int64_t nnz, const float* rhs, int64_t n_rhs_cols,
+                           float* out, void* workspace, int64_t workspace_bytes, void* stream);
+
+/* out = A rhs + (1 + epsilon) rhs (square A).  Replaces s_spmm_add_csr_int32
+ * (cbm/cbm_extensions.cpp:446-492). */
+int cbm_s_spmm_add_csr_int32(const int32_t* rp_b, const int32_t* rp_e, const int32_t* col, const float* val,
+                             int64_t n_rows, int64_t n_cols, int64_t nnz, const float* rhs, int64_t n_rhs_cols,
+                             float epsilon, float* out, void* workspace, int64_t workspace_bytes, void* stream);
+
+/* out = Delta rhs, then out[dst] += out[src] along the tree.  Replaces
+ * s_spmm_update_csr_int32 (cbm/cbm_extensions.cpp:351-444). */
+int cbm_s_spmm_update_csr_int32(const int32_t* rp_b, const int32_t* rp_e, const int32_t* col, const float* val,
+                                int64_t n_rows, int64_t n_cols, int64_t nnz, const float* rhs, int64_t n_rhs_cols,
+                                const int32_t* branches, int64_t n_branch_offsets, const int32_t* src,
+                                const int32_t* dst, int64_t n_edges, float* out, void* workspace,
+                                int64_t workspace_bytes, void* stream);
+
+/* out = Delta rhs, then out[dst] = fma(out[src], m[dst] / m[src], out[dst]).
+ * Replaces s_spmm_fused_update_csr_int32 (cbm/cbm_extensions.cpp:593-698). */
+int cbm_s_spmm_fused_update_csr_int32(const int32_t* rp_b, const int32_t* rp_e, const int32_t* col,
+                                      const float* val, int64_t n_rows, int64_t n_cols, int64_t nnz,
+                                      const float* rhs, int64_t n_rhs_cols, const int32_t* branches,
+                                      int64_t n_branch_offsets, const int32_t* src, const int32_t* dst,
+                                      int64_t n_edges, const float* multiplier, float* out, void* workspace,
+                                      int64_t workspace_bytes, void* stream);
+
+/* out = Delta rhs, the update, then out += (1 + epsilon) rhs (square A).
+ * Replaces s_spmm_update_add_csr_int32 (cbm/cbm_extensions.cpp:494-591). */
+int cbm_s_spmm_update_add_csr_int32(const int32_t* rp_b, const int32_t* rp_e, const int32_t* col,
+                                    const float* val, int64_t n_rows, int64_t n_cols, int64_t nnz,
+                                    const float* rhs, int64_t n_rhs_cols, float epsilon, const int32_t* branches,
+                                    int64_t n_branch_offsets, const int32_t* src, const int32_t* dst,
+                                    int64_t n_edges, float* out, void* workspace, int64_t workspace_bytes,
+                                    void* stream);
+
+/* out[dst] += out[src] along the tree, in place on out [n_out_rows,
+ * n_out_cols].  Replaces s_update_csr_int32 (cbm/cbm_extensions.cpp:784-838). */
+int cbm_s_update_csr_int32(const int32_t* branches, int64_t n_branch_offsets, const int32_t* src,
+                           const int32_t* dst, int64_t n_edges, float* out, int64_t n_out_rows,
+                           int64_t n_out_cols, void* workspace, int64_t workspace_bytes, void* stream);
+
+/* out[dst] = fma(out[src], m[dst] / m[src], out[dst]) along the tree, in place.
+ * Replaces s_fused_update_csr_int32 (cbm/cbm_extensions.cpp:841-907). */
+int cbm_s_fused_update_csr_int32(const int32_t* branches, int64_t n_branch_offsets, const int32_t* src,
+                                 const int32_t* dst, int64_t n_edges, const float* multiplier, float* out,
+                                 int64_t n_out_rows, int64_t n_out_cols, void* workspace, int64_t workspace_bytes,
+                                 void* stream);
 
 /* Plan statistics (for the bench's algorithmic byte counts). */
 enum {

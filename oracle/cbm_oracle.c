@@ -27,6 +27,11 @@
  *                         cbm/cbm_extensions.cpp:662-697)
  *   oracle_csr_spmm_f64   FP64 ground truth y = rs o (A (cs o x)), optionally
  *                         with A transposed
+ *   oracle_spmm_be, oracle_spmm_t_be, oracle_update_only, oracle_axpy
+ *                         the pieces of the reference's cbm_mkl_cpp products
+ *                         (cbm/cbm_extensions.cpp:351-907) on MKL's four-array
+ *                         CSR (begin/end row pointers): SpMM, transposed SpMM,
+ *                         the branch-serial update alone, and its cblas_saxpy
  * The *_omp variants parallelise the SpMM over rows and the update over
  * branches with OpenMP (schedule(dynamic, 50) as the reference's CPU path).
  */
@@ -321,6 +326,48 @@ void oracle_spmm_fused_update_omp(int64_t n_rows, int64_t c, const int32_t* rp, 
                                   const int32_t* src, const int32_t* dst, const float* m, float* y) {
   csr_spmm_f32(n_rows, c, rp, ci, val, x, y, 1);
   update(c, n_branches, br, src, dst, m, 2, y, 1);
+}
+
+/* ---- the cbm_mkl_cpp products' pieces (cbm/cbm_extensions.cpp:351-907) ---- */
+/* y[n_rows, c] = A x, row i's entries [rp_b[i], rp_e[i]) (MKL's four-array
+ * CSR, mkl_sparse_s_create_csr at :365-372), one FMA per entry in order */
+void oracle_spmm_be(int64_t n_rows, int64_t c, const int32_t* rp_b, const int32_t* rp_e, const int32_t* ci,
+                    const float* val, const float* x, float* y) {
+  for (int64_t i = 0; i < n_rows; ++i) {
+    float* yr = y + i * c;
+    for (int64_t q = 0; q < c; ++q) yr[q] = 0.0f;
+    for (int64_t k = rp_b[i]; k < rp_e[i]; ++k) {
+      const float a = val[k];
+      const float* xr = x + (int64_t)ci[k] * c;
+      for (int64_t q = 0; q < c; ++q) yr[q] = fmaf(a, xr[q], yr[q]);
+    }
+  }
+}
+
+/* y[n_cols, c] = A^T x (SPARSE_OPERATION_TRANSPOSE, :742-782): rows of A in
+ * order, each entry's term added with one FMA */
+void oracle_spmm_t_be(int64_t n_rows, int64_t n_cols, int64_t c, const int32_t* rp_b, const int32_t* rp_e,
+                      const int32_t* ci, const float* val, const float* x, float* y) {
+  memset(y, 0, sizeof(float) * n_cols * c);
+  for (int64_t i = 0; i < n_rows; ++i) {
+    const float* xr = x + i * c;
+    for (int64_t k = rp_b[i]; k < rp_e[i]; ++k) {
+      const float a = val[k];
+      float* yr = y + (int64_t)ci[k] * c;
+      for (int64_t q = 0; q < c; ++q) yr[q] = fmaf(a, xr[q], yr[q]);
+    }
+  }
+}
+
+/* the update alone, in place (:784-907): mode 0 plain, 2 the CPU fused rule */
+void oracle_update_only(int64_t c, int64_t n_branches, const int32_t* br, const int32_t* src, const int32_t* dst,
+                        const float* m, int mode, float* y) {
+  update(c, n_branches, br, src, dst, m, mode, y, 0);
+}
+
+/* y = (a x) + y element-wise with one FMA each: the cblas_saxpy of :490, :590 */
+void oracle_axpy(int64_t n, float a, const float* x, float* y) {
+  for (int64_t i = 0; i < n; ++i) y[i] = fmaf(a, x[i], y[i]);
 }
 
 int oracle_threads(void) {

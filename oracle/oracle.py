@@ -203,3 +203,89 @@ def degree_inv_sqrt(ptr):
 
 def threads():
     return int(lib().oracle_threads())
+
+
+# ---- the reference's cbm_mkl_cpp products (cbm/cbm_extensions.cpp:351-907) ------
+# Same names, argument order and in-place ``dst`` as the reference's operators,
+# on numpy arrays; each composes the C pieces as the reference composes MKL's
+# SpMM, the branch-serial update and cblas_saxpy.
+
+def _mkl_lib():
+    L = lib()
+    if not getattr(L, "_mkl_ready", False):
+        L.oracle_spmm_be.restype = None
+        L.oracle_spmm_be.argtypes = [i64, i64, vp, vp, vp, vp, vp, vp]
+        L.oracle_spmm_t_be.restype = None
+        L.oracle_spmm_t_be.argtypes = [i64, i64, i64, vp, vp, vp, vp, vp, vp]
+        L.oracle_update_only.restype = None
+        L.oracle_update_only.argtypes = [i64, i64, vp, vp, vp, vp, i32, vp]
+        L.oracle_axpy.restype = None
+        L.oracle_axpy.argtypes = [i64, C.c_float, vp, vp]
+        L._mkl_ready = True
+    return L
+
+
+def _out(dst):
+    if not (isinstance(dst, np.ndarray) and dst.dtype == np.float32 and dst.flags.c_contiguous and dst.ndim == 2):
+        raise TypeError("dst must be a C-contiguous float32 numpy matrix")
+    return dst
+
+
+def _spmm_into(rp_b, rp_e, col, val, rhs, dst):
+    rp_b, rp_e, col = _c(rp_b, np.int32), _c(rp_e, np.int32), _c(col, np.int32)
+    val, rhs = _c(val, np.float32), _c(rhs, np.float32)
+    _mkl_lib().oracle_spmm_be(dst.shape[0], dst.shape[1], rp_b.ctypes.data, rp_e.ctypes.data, col.ctypes.data,
+                              val.ctypes.data, rhs.ctypes.data, dst.ctypes.data)
+    return rhs
+
+
+def _update_into(branches, src, dst_idx, mult, mode, dst):
+    br, s, d = _c(branches, np.int32), _c(src, np.int32), _c(dst_idx, np.int32)
+    m = _c(mult, np.float32) if mult is not None else None
+    _mkl_lib().oracle_update_only(dst.shape[1], max(br.size - 1, 0), br.ctypes.data, s.ctypes.data, d.ctypes.data,
+                                  m.ctypes.data if m is not None else None, mode, dst.ctypes.data)
+
+
+def _axpy_into(a, rhs, dst):
+    _mkl_lib().oracle_axpy(dst.size, float(a), rhs.ctypes.data, dst.ctypes.data)
+
+
+def s_spmm_update_csr_int32(rp_b, rp_e, col, val, rhs, branches, src, dst_idx, dst):
+    _spmm_into(rp_b, rp_e, col, val, rhs, _out(dst))
+    _update_into(branches, src, dst_idx, None, 0, dst)
+
+
+def s_spmm_fused_update_csr_int32(rp_b, rp_e, col, val, rhs, branches, src, dst_idx, multiplier, dst):
+    _spmm_into(rp_b, rp_e, col, val, rhs, _out(dst))
+    _update_into(branches, src, dst_idx, multiplier, 2, dst)
+
+
+def s_spmm_add_csr_int32(rp_b, rp_e, col, val, rhs, eps, dst):
+    x = _spmm_into(rp_b, rp_e, col, val, rhs, _out(dst))
+    _axpy_into(np.float32(1.0) + np.float32(eps), x, dst)
+
+
+def s_spmm_update_add_csr_int32(rp_b, rp_e, col, val, rhs, eps, branches, src, dst_idx, dst):
+    x = _spmm_into(rp_b, rp_e, col, val, rhs, _out(dst))
+    _update_into(branches, src, dst_idx, None, 0, dst)
+    _axpy_into(np.float32(1.0) + np.float32(eps), x, dst)
+
+
+def s_spmm_csr_int32(rp_b, rp_e, col, val, rhs, dst):
+    _spmm_into(rp_b, rp_e, col, val, rhs, _out(dst))
+
+
+def s_spmm_csr_t_int32(rp_b, rp_e, col, val, rhs, dst):
+    rp_b, rp_e, col = _c(rp_b, np.int32), _c(rp_e, np.int32), _c(col, np.int32)
+    val, rhs = _c(val, np.float32), _c(rhs, np.float32)
+    _out(dst)
+    _mkl_lib().oracle_spmm_t_be(rp_b.size, dst.shape[0], dst.shape[1], rp_b.ctypes.data, rp_e.ctypes.data,
+                                col.ctypes.data, val.ctypes.data, rhs.ctypes.data, dst.ctypes.data)
+
+
+def s_update_csr_int32(branches, src, dst_idx, dst):
+    _update_into(branches, src, dst_idx, None, 0, _out(dst))
+
+
+def s_fused_update_csr_int32(branches, src, dst_idx, multiplier, dst):
+    _update_into(branches, src, dst_idx, multiplier, 2, _out(dst))
