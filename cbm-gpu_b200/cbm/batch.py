@@ -52,6 +52,10 @@ class cbm_batch:  # noqa: N801 (named like the other operator classes)
         cols, vals, br, src, dst = [], [], [np.zeros(1, np.int64)], [], []
         nnz = 0
         edges = 0
+        # where graph g's delta entries, tree edges and branch offsets start
+        self.nnz_offsets = [0]
+        self.edge_offsets = [0]
+        self.branch_offsets = [0]
         if sum(s.csr_col.size for s in parts) >= 2 ** 31:
             raise RuntimeError("a batch holds fewer than 2^31 delta entries")
         for g, s in enumerate(parts):
@@ -64,6 +68,9 @@ class cbm_batch:  # noqa: N801 (named like the other operator classes)
             dst.append(s.dst.astype(np.int64) + off)
             nnz += s.csr_col.size
             edges += s.src.size
+            self.nnz_offsets.append(nnz)
+            self.edge_offsets.append(edges)
+            self.branch_offsets.append(self.branch_offsets[-1] + s.branches.size - 1)
         self.nnz_a = int(sum(s.nnz_a for s in parts))
         crow = np.concatenate(crow).astype(np.int32)
         self.csr_ptr, self.csr_col = crow, np.concatenate(cols).astype(np.int32)
@@ -92,6 +99,18 @@ class cbm_batch:  # noqa: N801 (named like the other operator classes)
     def split(self, t):
         """Per-graph views of a [total nodes, C] tensor."""
         return [t[int(self.offsets[g]): int(self.offsets[g + 1])] for g in range(len(self.sizes))]
+
+    def graph_structure(self, g):
+        """Graph g's own CBM structure, indices rebased to the graph: (row_ptr,
+        col, val, branches, src, dst) as the reference's cbm_mkl_cpp.init and
+        its products take them."""
+        off = int(self.offsets[g])
+        z0, z1 = self.nnz_offsets[g], self.nnz_offsets[g + 1]
+        e0, e1 = self.edge_offsets[g], self.edge_offsets[g + 1]
+        b0, b1 = self.branch_offsets[g], self.branch_offsets[g + 1]
+        crow = self.csr_ptr[off:int(self.offsets[g + 1]) + 1].astype(np.int64) - z0
+        return (crow.astype(np.int32), self.csr_col[z0:z1] - off, self.csr_val[z0:z1],
+                self.branches[b0:b1 + 1] - e0, self.src[e0:e1] - off, self.dst[e0:e1] - off)
 
     def capture(self, x, y, warmup=2):
         """A CUDA graph that replays ``matmul(x, y)`` (x is read at replay time)."""
