@@ -8,25 +8,30 @@
 // plan's device layout) and cbm_matmul wants a caller-allocated workspace;
 // this entry point needs neither.  It reads the delta matrix and the tree in
 // the reference's own layout (CSR + BFS edge list) straight from the caller's
-// buffers and keeps its scratch (queue counters, a launch counter, and two
-// ready flags per row) in one fixed array compiled into this file.
+// buffers and keeps its scratch (queue counters, a status word, and per row a
+// parent mark and a ready flag) in one fixed array compiled into this file.
 //
 // The array is a file-scope __device__ variable, zero-filled when the module
 // loads: every GPU that loads this library holds its 8 MiB until the process
 // exits.  Calls share it and it keeps the last call's contents: every call
 // zeroes the queue counters before using them and clears the status word after
-// reporting it; the ready flags are compared against a per-call stamp, so they
-// need no clearing.  Calls
-// whose kernels overlap on the GPU (two streams, no ordering between them)
-// race on the array and give wrong results.  Host code cannot use the
-// array's name as a device address (on the host it names a host-side stand-in);
-// the device address is fetched once per device with cudaGetSymbolAddress,
-// with that device current, on the first call made on that device.
+// reporting it; the parent marks and ready flags are compared against a stamp
+// unique to the call (a process-wide counter on the host), so they need no
+// clearing, and a call that stopped half-way cannot leave marks that the next
+// call mistakes for its own.  Calls whose kernels overlap on the GPU (two
+// streams, no ordering between them) race on the array and give wrong
+// results.  Host code cannot use the array's name as a device address (on the
+// host it names a host-side stand-in); the device address is fetched once per
+// device with cudaGetSymbolAddress, with that device current, on the first
+// call made on that device, and kept for the life of the process: after a
+// cudaDeviceReset the module, and with it the array, is loaded anew at another
+// address, so this entry point must not be used after a device reset.
 //
 // Two kernels on the caller's stream:
 //   1. every row: Y[v] = sum_k val_k * X[col_k] (sequential FMAs per row, the
-//      order cbm_matmul uses for rows it does not split), and a mark on every
-//      node that has a parent;
+//      order cbm_matmul uses for rows it does not split; a row whose pointers
+//      are not 0 <= begin <= end <= nnz is recorded and written as zeros), and
+//      a mark on every node that has a parent (a second parent is recorded);
 //   2. every tree edge (u, v), in the given BFS order, taken from a work queue:
 //      wait (bounded) until u is final if u has a parent, then
 //      Y[v] += Y[u]   or   Y[v] += Y[u] * m[v] / m[u]   (cbm/cbm.cu:54, :88),
@@ -35,6 +40,7 @@
 #include "cbm_b200.h"
 #include "kernels.cuh"
 
+#include <atomic>
 #include <mutex>
 
 namespace {
@@ -80,8 +86,17 @@ struct NoAllocArgs {
   int64_t c;
   unsigned char* scratch;
   int32_t* status;
+  unsigned stamp;  // unique to the call: marks and flags equal to it are this call's
   long long timeout_ns;
 };
+
+std::atomic<unsigned> g_stamp{0};
+
+unsigned next_stamp() {
+  unsigned s = g_stamp.fetch_add(1u) + 1u;
+  if (s == 0) s = g_stamp.fetch_add(1u) + 1u;  // 0 is the zero-filled array's value
+  return s;
+}
 
 __device__ __forceinline__ cbm::QueueState* state(const NoAllocArgs& a) {
   return reinterpret_cast<cbm::QueueState*>(a.scratch);
@@ -100,7 +115,7 @@ __device__ void record(cbm::QueueState* qs, int code, long long info) {
 // Kernel 1: delta rows, warp per row, 128 columns per pass; parent marks.
 __global__ void __launch_bounds__(kWarps * 32) noalloc_rows(const NoAllocArgs a) {
   cbm::QueueState* qs = state(a);
-  const unsigned target = *(volatile unsigned*)&qs->epoch + 1u;
+  const unsigned target = a.stamp;
   const int lane = threadIdx.x & 31;
   const int64_t warp = (int64_t)blockIdx.x * kWarps + (threadIdx.x >> 5);
   const int64_t n_warps = (int64_t)gridDim.x * kWarps;
@@ -115,10 +130,15 @@ __global__ void __launch_bounds__(kWarps * 32) noalloc_rows(const NoAllocArgs a)
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < a.n_edges;
        e += (int64_t)gridDim.x * blockDim.x) {
     const int32_t v = a.dst[e];
-    if (v >= 0 && v < a.n_rows) hp[v] = target;
+    if (v >= 0 && v < a.n_rows && atomicExch(hp + v, target) == target) record(qs, CBM_ERR_STRUCTURE, e);
   }
+  const int64_t nnz = a.n_rows > 0 ? a.row_ptr[a.n_rows] : 0;
   for (int64_t row = warp; row < a.n_rows; row += n_warps) {
-    const int64_t b = a.row_ptr[row], e = a.row_ptr[row + 1];
+    int64_t b = a.row_ptr[row], e = a.row_ptr[row + 1];
+    if (b < 0 || e < b || e > nnz) {
+      if (lane == 0) record(qs, CBM_ERR_INDEX, row);
+      b = e = 0;  // the row is written as zeros
+    }
     for (int64_t c0 = 0; c0 < a.c; c0 += 128) {
       float acc[4] = {0.f, 0.f, 0.f, 0.f};
       for (int64_t base = b; base < e; base += 32) {
@@ -130,14 +150,14 @@ __global__ void __launch_bounds__(kWarps * 32) noalloc_rows(const NoAllocArgs a)
           val = a.values ? a.values[k] : 1.f;
           if (col < 0 || col >= a.n_cols) {
             record(qs, CBM_ERR_INDEX, k);
-            col = 0;
-            val = 0.f;
+            col = -1;  // skipped: nothing is read for it
           }
         }
         const int cnt = (int)((e - base) < 32 ? (e - base) : 32);
         for (int j = 0; j < cnt; ++j) {
           const int32_t cj = __shfl_sync(0xffffffffu, col, j);
           const float vj = __shfl_sync(0xffffffffu, val, j);
+          if (cj < 0) continue;
           const float* xr = a.x + (int64_t)cj * a.c;
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
@@ -158,7 +178,7 @@ __global__ void __launch_bounds__(kWarps * 32) noalloc_rows(const NoAllocArgs a)
 // Kernel 2: tree edges from a work queue, in the given order.
 __global__ void __launch_bounds__(kWarps * 32) noalloc_edges(const NoAllocArgs a) {
   cbm::QueueState* qs = state(a);
-  const unsigned target = *(volatile unsigned*)&qs->epoch + 1u;
+  const unsigned target = a.stamp;
   const int lane = threadIdx.x & 31;
   const unsigned* hp = has_parent(a);
   unsigned* rd = ready(a);
@@ -205,7 +225,6 @@ __global__ void __launch_bounds__(kWarps * 32) noalloc_edges(const NoAllocArgs a
       qs->next_row = 0;
       qs->done_blocks = 0;
       __threadfence();
-      atomicExch(&qs->epoch, target);
     }
   }
 }
@@ -249,6 +268,7 @@ extern "C" int cbm_matmul_noalloc(const int32_t* row_ptr, const int32_t* col_idx
   a.c = n_x_cols;
   a.scratch = static_cast<unsigned char*>(scratch);
   a.status = d_status;
+  a.stamp = next_stamp();
   a.timeout_ns = 1000000000ll;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   noalloc_rows<<<grid_of(reinterpret_cast<const void*>(noalloc_rows)), kWarps * 32, 0, st>>>(a);

@@ -271,9 +271,13 @@ int cbm_plan_error(cbm_plan* plan, void* stream, int32_t* device_status, int64_t
  * Scratch: a fixed 8 MiB array inside the library, held on every GPU that
  * loads it; n_rows above CBM_NOALLOC_MAX_ROWS returns CBM_ERR_TOO_LARGE.
  * The first call on a device looks up the array's device address (set-up);
- * make that first call before any stream capture.  Calls share the array:
- * calls whose kernels overlap on the GPU race.  Allocates nothing; two kernel
- * launches on `stream`, no synchronisation. */
+ * make that first call before any stream capture.  That address is kept for
+ * the life of the process: do not call this entry point after a
+ * cudaDeviceReset.  Calls share the array: calls whose kernels overlap on the
+ * GPU race.  Row pointers outside 0 <= begin <= end <= row_ptr[n_rows] and
+ * column or tree indices out of range are skipped and reported as
+ * CBM_ERR_INDEX, a node with two parents as CBM_ERR_STRUCTURE.  Allocates
+ * nothing; two kernel launches on `stream`, no synchronisation. */
 #define CBM_NOALLOC_MAX_ROWS 1048544
 int cbm_matmul_noalloc(const int32_t* row_ptr, const int32_t* col_idx, const float* values, int64_t n_rows,
                        int64_t n_cols, const int32_t* src, const int32_t* dst, int64_t n_edges,
