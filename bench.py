@@ -14,11 +14,21 @@ The line also carries "gcn": a 2-layer GCN (128 -> 256 -> 40) on the
 rows, seed 3), forward + backward ms per step with BF16 activations and with
 plain FP32, and their ratio (rank 0 only).
 
+At N = 1 the line also carries the other forms, each measured on the device
+with CUDA events after its own warm-up, outside the headline's timed region:
+"precision" (A D^-1/2 X on the 2.4M-node workload, X stored BF16), "batch"
+(the 512-graph workload in one launch replayed from a CUDA graph) and
+"reference_gpu" (the reference's own cusparseCBM.matmul_DAX_DADX, compiled
+from its source, on the headline's structure), with error against FP64 on
+sampled rows.
+
 N > 1 runs under torchrun, one rank per GPU: each rank owns a 256-column shard
 of X and Y (column sharding needs no collective; weak scaling).  Rank 0
 prints one JSON line.  ``--impl reference`` times the reference's CPU product
-path (CSR SpMM + branch-serial fused update, cbm/cbm_extensions.cpp:593-698) as
-restated by the oracle, on all host threads.
+path (MKL CSR SpMM + OpenMP branch-serial fused update,
+s_spmm_fused_update_csr_int32, cbm/cbm_extensions.cpp:593-698), compiled from
+its source into oracle/_ref/ (else the oracle's restatement of it), on all
+host threads.
 """
 from __future__ import annotations
 
@@ -58,6 +68,29 @@ def bytes_alg(n, z, e, b, cols, sx=4, sy=4, scaled=True):
     parent-row read, branch offsets, and the D^-1/2 vector."""
     return (4 * (n + 1) + 4 * z + z * cols * sx + n * cols * sy + e * (8 + 4 * cols) + 4 * (b + 1)
             + (4 * n if scaled else 0))
+
+
+def bytes_compulsory(n, z, e, b, cols, sx=4, sy=4, scaled=True):
+    """Bytes any implementation of one product must move: X read once, Y
+    written once, the delta matrix (row pointers, column indices; signs free),
+    the tree (ids per edge, branch offsets) and D^-1/2.  X-row gathers that
+    miss L2 are re-reads on top of these."""
+    return (n * cols * sx + n * cols * sy + 4 * (n + 1) + 4 * z + 8 * e + 4 * (b + 1) + (4 * n if scaled else 0))
+
+
+def roofline(b_alg, b_min, ms, traffic=None):
+    """Roofline record of one launch of ms milliseconds against the measured
+    HBM copy peak: the algorithmic (gather) rate, the compulsory-byte rate and,
+    given the DRAM bytes of an ncu capture, the DRAM rate."""
+    peak, kind = peaks()
+    t = ms * 1e-3
+    r = {"bound": "hbm", "achieved": b_alg / t / 1e9, "peak": peak, "unit": "GB/s", "frac": b_alg / t / 1e9 / peak,
+         "peak_kind": kind, "bytes_alg_per_launch": int(b_alg), "bytes_compulsory_per_launch": int(b_min),
+         "compulsory_achieved": b_min / t / 1e9, "frac_compulsory": b_min / t / 1e9 / peak, "traffic": traffic}
+    if traffic:
+        r["dram_achieved"] = traffic / t / 1e9
+        r["dram_frac"] = traffic / t / 1e9 / peak
+    return r
 
 
 def load_graph(rank, world):
@@ -165,37 +198,89 @@ class Clocks:
 
 
 def traffic_from_profile():
-    """DRAM bytes per launch of the product kernel from the committed ncu summary."""
-    path = os.path.join(REPO, "profiles", "fwd_kernel_powerlaw-1m.md")
+    """DRAM bytes per launch of the product kernel from the committed ncu
+    summary, and where they come from (the summary's file and the commit it
+    was captured at)."""
+    name = "fwd_stream_kernel_powerlaw-1m.md"
+    path = os.path.join(REPO, "profiles", name)
+    traffic, commit = None, None
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_launch:"):
-                return float(line.split(":", 1)[1].split()[0])
+                traffic = float(line.split(":", 1)[1].split()[0])
+            if line.startswith("commit:"):
+                commit = line.split(":", 1)[1].strip().split()[0]
     except OSError:
         pass
-    return None
+    return traffic, {"profile": f"profiles/{name}", "commit": commit}
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def reference_cpu_product():
+    """(run, kind, what): the reference's own CPU product
+    s_spmm_fused_update_csr_int32 (cbm/cbm_extensions.cpp:593-698: MKL
+    mkl_sparse_s_mm, then the OpenMP branch-parallel fused update), compiled
+    from its source into oracle/_ref/ by oracle/build_ref.py; where that module
+    is absent, the oracle's restatement of it (same arithmetic, plain loops).
+    run(crow, col, val, x, branches, src, dst, mult) computes one product on all
+    host threads."""
+    import torch as _t
+
+    from oracle import build_ref, oracle
+
+    mod = build_ref.load(build_ref.CPU_MODULE)
+    if mod is not None:
+        cache = {}
+
+        def run(crow, col, val, x, br, src, dst, mult):
+            key = id(crow), id(x)
+            if key not in cache:
+                cache.clear()
+                ct = _t.from_numpy(np.ascontiguousarray(crow, dtype=np.int32))
+                cache[key] = ([ct[:-1].clone(), ct[1:].clone()] +
+                              [_t.from_numpy(np.ascontiguousarray(a, dtype=d)) for a, d in
+                               ((col, np.int32), (val, np.float32), (x, np.float32), (br, np.int32),
+                                (src, np.int32), (dst, np.int32), (mult, np.float32))] +
+                              [_t.empty(x.shape, dtype=_t.float32)])
+            a = cache[key]
+            mod.s_spmm_fused_update_csr_int32(*a)
+            return a[-1]
+
+        return run, "reference", "the reference's s_spmm_fused_update_csr_int32 (MKL + OpenMP), built from its source"
+
+    def run(crow, col, val, x, br, src, dst, mult):
+        return oracle.spmm_fused_update(crow, col, val, x, br, src, dst, mult, gpu_order=False, parallel=True)
+
+    return run, "port", "the oracle's restatement of s_spmm_fused_update_csr_int32 (OpenMP)"
 
 
 def cpu_baseline(a, x_np, b_alg, budget_s=15.0):
-    """The reference's CPU product path (oracle port, all threads) on the same workload."""
-    from oracle import oracle
-
+    """The reference's CPU product path on all host threads, on the same workload."""
     crow = a.deltas.crow_indices().cpu().numpy()
     col = a.deltas.col_indices().cpu().numpy()
     val = a.deltas.values().cpu().numpy()
     br, src, dst = (t.cpu().numpy() for t in (a.mca_offset, a.mca_src_idx, a.mca_dst_idx))
     mult = a.D.cpu().numpy()
+    run, kind, what = reference_cpu_product()
+    run(crow, col, val, x_np, br, src, dst, mult)  # warm-up (first-touch, MKL set-up)
     times = []
     t_end = time.perf_counter() + budget_s
     while not times or time.perf_counter() < t_end:
         t0 = time.perf_counter()
-        oracle.spmm_fused_update(crow, col, val, x_np, br, src, dst, mult, parallel=True)
+        run(crow, col, val, x_np, br, src, dst, mult)
         times.append(time.perf_counter() - t0)
-        if len(times) >= 5:
+        if len(times) >= 10:
             break
     t = statistics.median(times)
-    return {"value": b_alg / t / 1e9, "unit": "GB/s", "cores": oracle.threads(), "kind": "port",
-            "sample": f"{len(times)} full products (median {t:.2f} s) of the same workload on the host CPU"}
+    return {"value": b_alg / t / 1e9, "unit": "GB/s", "cores": host_threads(), "kind": kind,
+            "ms_per_product": t * 1e3,
+            "sample": f"{len(times)} full products (median {t:.3f} s) of the same workload: {what}"}
 
 
 def run_reference(args, rank, world):
@@ -216,23 +301,22 @@ def run_reference(args, rank, world):
     x = np.random.default_rng(1).standard_normal((n, COLS), dtype=np.float32)
     z, e, b = int(col.size), int(s.src.size), int(s.branches.size) - 1
     b_alg = bytes_alg(n, z, e, b, COLS)
+    run, kind, what = reference_cpu_product()
     for _ in range(args.warmup):
-        oracle.spmm_fused_update(crow, col, val, x, s.branches, s.src, s.dst, dinv, parallel=True)
+        run(crow, col, val, x, s.branches, s.src, s.dst, dinv)
     ts = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        oracle.spmm_fused_update(crow, col, val, x, s.branches, s.src, s.dst, dinv, parallel=True)
+        run(crow, col, val, x, s.branches, s.src, s.dst, dinv)
         ts.append(time.perf_counter() - t0)
     t = sum(ts) / len(ts)
     v = b_alg / t / 1e9
-    cores = oracle.threads()
     line = {"impl": "reference", "metric": "CBM DAD.X GB/s (algorithmic bytes)", "value": v, "unit": "GB/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "config": config_dict(n, s.nnz_a, z, e, b, world),
-            "cpu_baseline": {"value": v, "unit": "GB/s", "cores": cores, "kind": "port",
-                             "sample": "every step one full product of the workload (oracle port of "
-                                       "s_spmm_fused_update_csr_int32, OpenMP)"},
+            "cpu_baseline": {"value": v, "unit": "GB/s", "cores": host_threads(), "kind": kind,
+                             "sample": f"every step one full product of the workload: {what}"},
             "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -291,10 +375,16 @@ def _time_events(fn, steps, warmup):
     return e0.elapsed_time(e1) / steps
 
 
-def run_batch(args):
+BATCH_SPACE = {"chunk_nnz": [128, 256], "rows_per_claim": [2, 4, 8], "variant": ["auto", "register"], "team": [0, 8]}
+PREC_SPACE = {"chunk_nnz": [256, 512], "rows_per_claim": [4, 8, 16], "variant": ["auto", "register", "tma"],
+              "hot_rows": [65536, 262144]}
+
+
+def batch_form(steps, warmup, space=None):
     """Batching form: 512 community graphs (log-uniform 1,000..64,000 nodes, mean
     degree U[8, 40], seed 4) in one launch replayed from a CUDA graph;
-    D^-1/2 A D^-1/2 X with X [sum N, 64] BF16, Y FP32; autotuned."""
+    D^-1/2 A D^-1/2 X with X [sum N, 64] BF16, Y FP32; launch knobs autotuned
+    over ``space``."""
     from cbm import _lib, synthetic
     from cbm.batch import cbm_batch
     from cbm.tune import autotune
@@ -307,44 +397,53 @@ def run_batch(args):
     g = torch.Generator(device="cuda").manual_seed(4)
     x = torch.randn(n, 64, device="cuda", generator=g).to(torch.bfloat16)
     y = torch.empty(n, 64, device="cuda")
-    tuned = autotune(b.plan, "dadx", x, y, space={"chunk_nnz": [128, 256], "rows_per_claim": [2, 4, 8],
-                                                  "variant": ["auto", "register"], "team": [0, 8]})
+    tuned = autotune(b.plan, "dadx", x, y, space=space or BATCH_SPACE)
     graph = b.capture(x, y)
     l0 = b.plan.stat(_lib.P_LAUNCHES)
-    ms = _time_events(graph.replay, args.steps, args.warmup)
+    ms = _time_events(graph.replay, steps, warmup)
+    launches = (b.plan.stat(_lib.P_LAUNCHES) - l0) / steps
     st = b.plan.stats
     b_alg = bytes_alg(n, st["nnz"], st["edges"], st["branches"], 64, sx=2, sy=4)
-    line = {"metric": "CBM batched DAD.X GB/s (algorithmic bytes)", "value": b_alg / (ms * 1e-3) / 1e9,
-            "unit": "GB/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-            "higher_is_better": True, "dtype": "bf16 X, f32 Y, f32 accumulate", "data": "synthetic",
-            "config": {"workload": "512 community graphs, one launch under a CUDA graph", "graphs": len(graphs),
-                       "nodes": n, "nnz_a": b.nnz_a, "nnz_delta": st["nnz"], "tree_edges": st["edges"],
-                       "cols": 64, "setup_s": setup_s},
-            "graphs_per_s": len(graphs) / (ms * 1e-3), "rows_per_s": n / (ms * 1e-3),
-            "launches_per_step": (b.plan.stat(_lib.P_LAUNCHES) - l0) / args.steps,
-            "autotune_best": {"config": tuned[0][0], "ms": tuned[0][1]},
-            "roofline": {"bound": "hbm", "achieved": b_alg / (ms * 1e-3) / 1e9, "peak": peaks()[0], "unit": "GB/s",
-                         "frac": b_alg / (ms * 1e-3) / 1e9 / peaks()[0], "peak_kind": peaks()[1]}}
+    b_min = bytes_compulsory(n, st["nnz"], st["edges"], st["branches"], 64, sx=2, sy=4)
     offs = b.offsets
     packed = np.concatenate([np.asarray(ei, dtype=np.int64) + int(offs[i]) for i, (ei, _) in enumerate(graphs)],
                             axis=1)
     dinv = dinv_f64(packed, n)
-    line["error_vs_fp64"] = fp64_sample_error(packed, n, x, y, rs=dinv, cs=dinv)
+    err = fp64_sample_error(packed, n, x, y, rs=dinv, cs=dinv)
     b.plan.check_device()
+    del graph
+    return {"metric": "CBM batched DAD.X GB/s (algorithmic bytes)", "value": b_alg / (ms * 1e-3) / 1e9,
+            "unit": "GB/s", "ms": ms, "steps": steps, "warmup": warmup,
+            "dtype": "bf16 X, f32 Y, f32 accumulate",
+            "config": {"workload": "512 community graphs, one launch under a CUDA graph", "graphs": len(graphs),
+                       "nodes": n, "nnz_a": b.nnz_a, "nnz_delta": st["nnz"], "tree_edges": st["edges"],
+                       "cols": 64, "setup_s": setup_s},
+            "graphs_per_s": len(graphs) / (ms * 1e-3), "rows_per_s": n / (ms * 1e-3),
+            "launches_per_step": launches, "autotune_best": {"config": tuned[0][0], "ms": tuned[0][1]},
+            "roofline": roofline(b_alg, b_min, ms), "error_vs_fp64": err}
+
+
+def run_batch(args):
+    r = batch_form(args.steps, args.warmup)
+    line = {"metric": r.pop("metric"), "value": r.pop("value"), "unit": r.pop("unit"), "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": r.pop("ms"), "higher_is_better": True,
+            "data": "synthetic"}
+    line.update(r)
     print(json.dumps(line), flush=True)
 
 
-def run_precision(args):
+def precision_form(steps, warmup, prec_nodes=0, space=None, knobs=None):
     """Precision form: A D^-1/2 X on the 2,400,000-node power-law graph
     (exponent 2.3, mean degree 50, 40% near-duplicate rows with 5% flips, seed 2,
-    alpha 16); X [N, 128] stored BF16, FP32 accumulation and output."""
-    from cbm import _lib, synthetic
+    alpha 16); X [N, 128] stored BF16, FP32 accumulation and output.  Launch
+    knobs from ``knobs`` or autotuned over ``space``."""
+    from cbm import synthetic
     from cbm.cbm4ad import cbm4ad
 
     t0 = time.time()
-    if args.prec_nodes:
+    if prec_nodes:
         # the same law at another size (profiling runs)
-        n = args.prec_nodes
+        n = prec_nodes
         ei = synthetic._w_powerlaw(n, 2.3, 50.0, 0.40, 0.05, 2)
         spec = {"alpha": 16}
     else:
@@ -355,37 +454,70 @@ def run_precision(args):
     x32 = torch.randn(n, 128, device="cuda", generator=g)
     x = x32.to(torch.bfloat16)
     y = torch.empty(n, 128, device="cuda")
-    if args.no_autotune:
-        a.plan.tune(chunk_nnz=args.chunk_nnz, rows_per_claim=args.rows_per_claim, variant=args.variant,
-                    hot_rows=args.hot_rows, team=args.team)
-        tuned = None
+    tuned = None
+    if knobs is not None:
+        a.plan.tune(**knobs)
     else:
         from cbm.tune import autotune
 
-        tuned = autotune(a.plan, "adx", x, y, space={"chunk_nnz": [256, 512], "rows_per_claim": [4, 8, 16],
-                                                     "variant": ["auto", "register", "tma"],
-                                                     "hot_rows": [65536, 262144]})
-    ms = _time_events(lambda: a.matmul(x, y), args.steps, args.warmup)
+        tuned = autotune(a.plan, "adx", x, y, space=space or PREC_SPACE)
+    ms = _time_events(lambda: a.matmul(x, y), steps, warmup)
     dinv = dinv_f64(ei, n)
     err = {"product": fp64_sample_error(ei, n, x, y, cs=dinv),
            "end_to_end": fp64_sample_error(ei, n, x32, y, cs=dinv)}
     st = a.plan.stats
     b_alg = bytes_alg(n, st["nnz"], st["edges"], st["branches"], 128, sx=2, sy=4)
-    line = {"metric": "CBM A.D^-1/2.X GB/s (algorithmic bytes), BF16 X", "value": b_alg / (ms * 1e-3) / 1e9,
-            "unit": "GB/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-            "higher_is_better": True, "dtype": "bf16 X, f32 Y, f32 accumulate", "data": "synthetic",
-            "config": {"workload": f"powerlaw (exponent 2.3, mean degree 50, 40% near-duplicates) N={n} A D^-1/2 X",
-                       "nodes": n,
-                       "nnz_a": a.structure_stats["nnz_a"], "nnz_delta": st["nnz"], "tree_edges": st["edges"],
-                       "cols": 128, "alpha": spec["alpha"], "setup_s": setup_s},
-            "rows_per_s": n / (ms * 1e-3),
-            "roofline": {"bound": "hbm", "achieved": b_alg / (ms * 1e-3) / 1e9, "peak": peaks()[0], "unit": "GB/s",
-                         "frac": b_alg / (ms * 1e-3) / 1e9 / peaks()[0], "peak_kind": peaks()[1]},
-            "plan": st,
-            "autotune_best": {"config": tuned[0][0], "ms": tuned[0][1]} if tuned else None,
-            "error_vs_fp64": err}
+    b_min = bytes_compulsory(n, st["nnz"], st["edges"], st["branches"], 128, sx=2, sy=4)
     a.plan.check_device()
+    return {"metric": "CBM A.D^-1/2.X GB/s (algorithmic bytes), BF16 X", "value": b_alg / (ms * 1e-3) / 1e9,
+            "unit": "GB/s", "ms": ms, "steps": steps, "warmup": warmup,
+            "dtype": "bf16 X, f32 Y, f32 accumulate",
+            "config": {"workload": f"powerlaw (exponent 2.3, mean degree 50, 40% near-duplicates) N={n} A D^-1/2 X",
+                       "nodes": n, "nnz_a": a.structure_stats["nnz_a"], "nnz_delta": st["nnz"],
+                       "tree_edges": st["edges"], "cols": 128, "alpha": spec["alpha"], "setup_s": setup_s},
+            "rows_per_s": n / (ms * 1e-3), "roofline": roofline(b_alg, b_min, ms), "plan": st,
+            "autotune_best": {"config": tuned[0][0], "ms": tuned[0][1]} if tuned else {"config": knobs},
+            "error_vs_fp64": err}
+
+
+def run_precision(args):
+    knobs = None
+    if args.no_autotune:
+        knobs = dict(chunk_nnz=args.chunk_nnz, rows_per_claim=args.rows_per_claim, variant=args.variant,
+                     hot_rows=args.hot_rows, team=args.team)
+    r = precision_form(args.steps, args.warmup, prec_nodes=args.prec_nodes, knobs=knobs)
+    line = {"metric": r.pop("metric"), "value": r.pop("value"), "unit": r.pop("unit"), "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": r.pop("ms"), "higher_is_better": True,
+            "data": "synthetic"}
+    line.update(r)
     print(json.dumps(line), flush=True)
+
+
+def reference_gpu_form(a, x, y_ours, steps, warmup):
+    """The reference's own GPU product cusparseCBM.matmul_DAX_DADX (cbm/cbm.cu:210-268:
+    cuSPARSE SpMM, then its fused_update kernel), compiled from its source into
+    oracle/_ref/, on the headline's structure and X: ms per product, its
+    algorithmic-byte rate, and its agreement with this library's result
+    (rtol 1e-5, atol 1e-6)."""
+    from oracle import build_ref
+
+    mod = build_ref.load("cbm_cusparse_ref")
+    if mod is None:
+        return {"unavailable": "the reference's GPU module was not built (no reference tree at build time)"}
+    n = a.num_nodes
+    br = a.mca_offset
+    # the reference's update kernel reads one branch offset past the end
+    # (one block per entry of mca_branches, cbm/cbm.cu:136, :193): hand it a
+    # view of a buffer with a readable sentinel equal to the edge count
+    br_pad = torch.cat([br, br[-1:]])[: br.numel()]
+    csr = torch.sparse_csr_tensor(a.deltas.crow_indices(), a.deltas.col_indices(), a.deltas.values(), (n, n))
+    ref = mod.cusparseCBM(csr, br_pad, a.mca_src_idx, a.mca_dst_idx, a.D)
+    y = torch.empty_like(x)
+    ms = _time_events(lambda: ref.matmul_DAX_DADX(x, y), steps, warmup)
+    agree = bool(torch.allclose(y, y_ours, rtol=1e-5, atol=1e-6))
+    del ref
+    return {"impl": "reference cusparseCBM.matmul_DAX_DADX (cbm/cbm.cu), built from its source for sm_100a",
+            "ms": ms, "steps": steps, "warmup": warmup, "agrees_rtol1e-5_atol1e-6": agree}
 
 
 def run_lsh(args):
@@ -435,6 +567,15 @@ def run_lsh(args):
     print(json.dumps(line), flush=True)
 
 
+def _form(fn):
+    """One of the other forms' records; a failure is recorded, not raised, so
+    that the headline line still prints."""
+    try:
+        return fn()
+    except Exception as exc:  # recorded in the line for the reader
+        return {"error": f"{type(exc).__name__}: {exc}"}
+
+
 def config_dict(n, nnz_a, z, e, b, world):
     return {"workload": f"{WORKLOAD}: D^-1/2 A D^-1/2 X fp32, power-law N={n}, alpha=8, C={COLS} per GPU",
             "nodes": n, "nnz_a": nnz_a, "nnz_delta": z, "tree_edges": e, "branches": b, "cols_per_gpu": COLS,
@@ -449,6 +590,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-gcn", action="store_true")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="leave the precision, batch and reference-GPU records out of the headline line")
     ap.add_argument("--gcn-only", action="store_true", help="only the GCN timing (one JSON object)")
     ap.add_argument("--workload", default="headline", choices=["headline", "batch", "precision", "lsh"],
                     help="batch / precision / lsh: the batching, precision or LSH-clustered form instead of "
@@ -562,10 +705,12 @@ def main():
     e2e_ms = max_over_ranks(e0.elapsed_time(e1) / e2e_steps, dev)
 
     if rank == 0:
-        peak, peak_kind = peaks()
         kernel_ms = statistics.mean(per)
-        achieved = b_alg / (kernel_ms * 1e-3) / 1e9
-        traffic = traffic_from_profile()
+        traffic, traffic_src = traffic_from_profile()
+        rl = roofline(b_alg, bytes_compulsory(n, z, e, b, COLS), kernel_ms, traffic)
+        rl["kernel"] = ("cbm::fwd_kernel<float,float,2,4>" if args.variant == "register"
+                        else "cbm::fwd_stream_kernel<float,float,32,2,4,8,128>")
+        rl["traffic_source"] = traffic_src
         line = {
             "metric": "CBM DAD.X GB/s (algorithmic bytes)",
             "value": b_alg * world / (ms_max * 1e-3) / 1e9,
@@ -581,13 +726,7 @@ def main():
             "data": "synthetic",
             "config": config_dict(n, a.structure_stats["nnz_a"], z, e, b, world),
             "rows_per_s": n * world / (ms_max * 1e-3),
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
-                         "dram_achieved": traffic / (kernel_ms * 1e-3) / 1e9 if traffic else None,
-                         "dram_frac": traffic / (kernel_ms * 1e-3) / 1e9 / peak if traffic else None,
-                         "kernel": ("cbm::fwd_kernel<float,float,2,4>" if args.variant == "register"
-                                    else "cbm::fwd_stream_kernel<float,float,32,2,4,8,128>"),
-                         "bytes_alg_per_launch": b_alg},
+            "roofline": rl,
             "e2e": {"value": b_alg * world / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s",
                     "h2d_bytes_per_step": int(xh.numel() * 4), "d2h_bytes_per_step": int(yh.numel() * 4),
                     "ms_per_step": e2e_ms, "api": "cbm4dad.matmul_host (pinned host X and Y)",
@@ -597,10 +736,27 @@ def main():
             "plan": a.plan.stats,
             "error_vs_fp64": err,
         }
+        if world == 1 and not args.no_forms:
+            line["reference_gpu"] = _form(lambda: reference_gpu_form(a, x, y, max(args.steps, 10), args.warmup))
+            if "ms" in line["reference_gpu"]:
+                r = line["reference_gpu"]
+                r["value"] = b_alg / (r["ms"] * 1e-3) / 1e9
+                r["unit"] = "GB/s"
+                r["ours_ms"] = kernel_ms
+                r["speedup_ours_over_reference"] = r["ms"] / kernel_ms
         if not args.no_gcn:
             line["gcn"] = gcn_timing(max(args.steps, 10), max(args.warmup, 3))
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(a, x.cpu().numpy(), b_alg)
+        if world == 1 and not args.no_forms:
+            del xh, yh, x, y, a
+            torch.cuda.empty_cache()
+            line["precision"] = _form(lambda: precision_form(max(args.steps, 10), args.warmup,
+                                                             space={"chunk_nnz": [256, 512],
+                                                                    "rows_per_claim": [8, 16]}))
+            torch.cuda.empty_cache()
+            line["batch"] = _form(lambda: batch_form(max(args.steps, 10), args.warmup,
+                                                     space={"rows_per_claim": [2, 4, 8]}))
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.barrier()
