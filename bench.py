@@ -357,7 +357,27 @@ def gcn_timing(steps, warmup):
         torch.cuda.synchronize()
         out[f"{name}_ms"] = e0.elapsed_time(e1) / steps
         out[f"{name}_cbm_launches_per_step"] = (a.plan.stat(_lib.P_LAUNCHES) - l0) / steps
+        # the step's CBM work alone: Ahat X (128 columns), Ahat (H W2) (40 columns,
+        # FP32 out) and the adjoint of the latter, on the step's dtypes
+        x_act = xin
+        y128 = torch.empty(n, 128, dtype=dt, device="cuda")
+        hw = torch.randn(n, 40, device="cuda", generator=g).to(dt)
+        y40 = torch.empty(n, 40, device="cuda")
+        g40 = torch.randn(n, 40, device="cuda", generator=g)
+        dx40 = torch.empty(n, 40, dtype=dt, device="cuda")
+
+        def cbm_work():
+            a.matmul(x_act, y128)
+            a.matmul(hw, y40)
+            a.adjoint(g40, dx40)
+
+        out[f"{name}_cbm_ms"] = _time_events(cbm_work, steps, warmup)
+        out[f"{name}_cbm_parts_ms"] = {
+            "ahat_x_128": _time_events(lambda: a.matmul(x_act, y128), steps, warmup),
+            "ahat_hw_40": _time_events(lambda: a.matmul(hw, y40), steps, warmup),
+            "adjoint_40": _time_events(lambda: a.adjoint(g40, dx40), steps, warmup)}
     out["speedup_bf16_over_fp32"] = out["fp32_ms"] / out["bf16_ms"]
+    out["cbm_speedup_bf16_over_fp32"] = out["fp32_cbm_ms"] / out["bf16_cbm_ms"]
     a.plan.check_device()
     return out
 

@@ -20,6 +20,7 @@ F32, BF16 = 0, 1
 OP_AX, OP_ADX, OP_DADX, OP_VALUES_ADD, OP_VALUES_RATIO, OP_DAD_ADD, OP_GIN = range(7)
 INPUT_DEVICE, INPUT_HOST = 0, 1
 VARIANT_AUTO, VARIANT_REGISTER, VARIANT_STAGED, VARIANT_TMA = 0, 1, 2, 3
+PASSES_AUTO, PASSES_FUSED, PASSES_TWO = 0, 1, 2
 BUILD_EXHAUSTIVE = 1
 COALESCE_SYMMETRIZE, COALESCE_DROP_SELF = 1, 2
 S_DELTA_ROW, S_DELTA_COL, S_DELTA_VAL, S_BRANCHES, S_SRC, S_DST, S_PARENT, S_CSR_PTR, S_CSR_COL, \
@@ -52,6 +53,7 @@ SIGNATURES = [
     ("cbm_matmul_gin", C.c_int, [vp, C.c_float, vp, i32, i64, vp, i32, i64, i64, vp, i64, vp]),
     ("cbm_plan_prepare_adjoint", C.c_int, [vp, vp]),
     ("cbm_plan_set_timeout", C.c_int, [vp, i64]),
+    ("cbm_plan_set_passes", C.c_int, [vp, i32]),
     ("cbm_plan_set_compensation", C.c_int, [vp, i32]),
     ("cbm_plan_debug_set_parent", C.c_int, [vp, i64, i32, vp]),
     ("cbm_plan_debug_check_transpose", C.c_int, [vp, vp]),

@@ -114,6 +114,12 @@ class Plan:
         _lib.check(self._lib.cbm_plan_set_compensation(self._h, int(min_depth)), "cbm_plan_set_compensation")
         self._ws.clear()
 
+    def set_passes(self, passes):
+        """'auto', 'fused' or 'two': one fused pass, or a delta pass then a
+        propagation pass (FP32 Y); bit-identical results."""
+        v = {"auto": _lib.PASSES_AUTO, "fused": _lib.PASSES_FUSED, "two": _lib.PASSES_TWO}[passes]
+        _lib.check(self._lib.cbm_plan_set_passes(self._h, v), "cbm_plan_set_passes")
+
     def set_timeout(self, ns):
         _lib.check(self._lib.cbm_plan_set_timeout(self._h, int(ns)), "cbm_plan_set_timeout")
 

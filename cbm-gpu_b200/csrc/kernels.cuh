@@ -111,6 +111,10 @@ struct FwdArgs {
   // as with BF16 Y
   int32_t gin;
   float gin_scale;
+  // first pass of a two-pass product (FP32 Y): rows store their delta sums
+  // only (no parent term, no ready flags); prop_kernel adds the parents
+  int32_t skip_parent;
+  int32_t publish_epoch;  // the last block publishes the launch epoch (0: a pass that another follows)
   long long timeout_ns;
 };
 
@@ -409,7 +413,7 @@ __device__ __forceinline__ void fwd_row(const FwdArgs& a, int item, unsigned epo
       }
     }
   }
-  const int p = a.par[item];
+  const int p = a.skip_parent ? -1 : a.par[item];
   // compensated arithmetic for this row, a residual to read from the parent
   const bool cmode = COMP && item >= a.comp_item0;
   const bool cread = COMP && item >= a.comp_read0;
@@ -498,7 +502,7 @@ __device__ __forceinline__ void fwd_row(const FwdArgs& a, int item, unsigned epo
       store_vec<YT, V>(yrow + (int64_t)vi * V, out);
     }
   }
-  if (internal) {
+  if (internal && !a.skip_parent) {
     if (sizeof(YT) != 4 || a.gin) {
       float* srow = a.pstate + (int64_t)a.self_slot[item] * a.ldp;
 #pragma unroll
@@ -513,7 +517,9 @@ __device__ __forceinline__ void fwd_row(const FwdArgs& a, int item, unsigned epo
   }
 }
 
-__device__ __forceinline__ void finish_block(QueueState* qs, unsigned epoch) {
+// The last block to finish resets the queue counters and, unless another pass
+// of the same product follows, publishes the launch epoch.
+__device__ __forceinline__ void finish_block(QueueState* qs, unsigned epoch, bool publish = true) {
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
@@ -523,7 +529,7 @@ __device__ __forceinline__ void finish_block(QueueState* qs, unsigned epoch) {
       qs->next_row = 0;
       qs->done_blocks = 0;
       __threadfence();
-      atomicExch(&qs->epoch, epoch);
+      if (publish) atomicExch(&qs->epoch, epoch);
     }
   }
 }
@@ -563,6 +569,95 @@ __global__ void __launch_bounds__(kThreads) fwd_kernel(const FwdArgs a) {
       const unsigned item = base + team + (unsigned)(r * teams);
       if (item >= (unsigned)a.n_items) break;
       fwd_row<XT, YT, VPL, V, COMP>(a, (int)item, epoch, tl, TL, tmask);
+    }
+    __syncwarp();
+  }
+  finish_block(a.qs, epoch, a.publish_epoch != 0);
+}
+
+// ============================================================================
+// Second pass of a two-pass product (FP32 Y): the first pass (fwd_kernel or
+// fwd_stream_kernel with skip_parent) left every row's delta sum in Y; this
+// pass adds the parent term to the rows below tree level 0, in level order
+// (items [n_root, n_items)): wait (bounded) until the parent is final when it
+// is itself below level 0, then
+//   Y[v] = Y[v] + Y[u]                 (PROP_ADD)
+//   Y[v] = Y[v] + (Y[u] m[v]) / m[u]   (PROP_RATIO, cbm/cbm.cu:88)
+// the same additions, in the same order, as the one-pass kernels, so results
+// are bit-identical.  A deep tree's rows then gather X without waiting on
+// their parents, and the waits left here are short (no gathers behind them).
+// ============================================================================
+struct PropArgs {
+  int32_t n_items;
+  int32_t n_root;
+  const int32_t* node;
+  const int32_t* par;
+  const int32_t* par_item;
+  float* y;
+  int64_t ldy;
+  int32_t nvec;
+  const float* mult;
+  int32_t prop_mode;
+  unsigned int* node_flag;
+  QueueState* qs;
+  int32_t team;
+  long long timeout_ns;
+};
+
+template <int VPL, int V>
+__global__ void __launch_bounds__(kThreads) prop_kernel(const PropArgs a) {
+  const int lane = threadIdx.x & 31;
+  const int TL = a.team;
+  const int team = lane / TL;
+  const int tl = lane & (TL - 1);
+  const int teams = 32 / TL;
+  const unsigned tmask = (TL == 32) ? 0xffffffffu : (((1u << TL) - 1u) << (team * TL));
+  const unsigned epoch = *(volatile unsigned*)&a.qs->epoch + 1u;
+  const unsigned n_deep = (unsigned)(a.n_items - a.n_root);
+  for (;;) {
+    unsigned base = 0;
+    if (lane == 0) base = atomicAdd(&a.qs->next_row, (unsigned)teams);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= n_deep) break;
+    const unsigned k = base + team;
+    if (k < n_deep) {
+      const int item = a.n_root + (int)k;
+      const int nodew = a.node[item];
+      const int node = nodew & 0x7fffffff;
+      const int p = a.par[item];
+      bool ok = p >= 0;
+      if (ok && a.par_item[item] >= a.n_root)
+        ok = wait_flag(a.node_flag + p, epoch, a.qs, a.timeout_ns, (long long)node);
+      if (ok) {
+        const bool ratio = a.prop_mode == PROP_RATIO;
+        const float dv = ratio ? __ldg(a.mult + node) : 1.f;
+        const float dp = ratio ? __ldg(a.mult + p) : 1.f;
+        const float* yp_row = a.y + (int64_t)p * a.ldy;
+        float* yv_row = a.y + (int64_t)node * a.ldy;
+#pragma unroll
+        for (int v = 0; v < VPL; ++v) {
+          const int vi = tl + v * TL;
+          if (vi < a.nvec) {
+            float yp[V], yv[V];
+            load_f32_cg<V>(yp_row + vi * V, yp);
+            load_f32_cg<V>(yv_row + vi * V, yv);
+            if (ratio) {
+#pragma unroll
+              for (int q = 0; q < V; ++q) yv[q] = __fadd_rn(yv[q], __fdiv_rn(__fmul_rn(yp[q], dv), dp));
+            } else {
+#pragma unroll
+              for (int q = 0; q < V; ++q) yv[q] = __fadd_rn(yv[q], yp[q]);
+            }
+            store_f32<V>(yv_row + vi * V, yv);
+          }
+        }
+      }
+      if (nodew < 0) {
+        // marked final even after a failed wait, so that no wait on it hangs
+        __threadfence();
+        __syncwarp(tmask);
+        if (tl == 0) st_release(a.node_flag + node, epoch);
+      }
     }
     __syncwarp();
   }
@@ -1131,7 +1226,7 @@ __global__ void __launch_bounds__(BLOCK) fwd_stream_kernel(const FwdArgs a, cons
       if (tl < nit) {
         const int64_t it = i0 + tl;
         m_node = a.node[it];
-        m_par = a.par[it];
+        m_par = a.skip_parent ? -1 : a.par[it];
         dep_in_claim = m_par >= 0 && a.par_item[it] >= (int)base;
         m_chunk = a.chunk0[it];
         m_pslot = a.par_slot[it];
@@ -1233,8 +1328,9 @@ __global__ void __launch_bounds__(BLOCK) fwd_stream_kernel(const FwdArgs a, cons
           }
         }
         YT* yrow = static_cast<YT*>(a.y) + (int64_t)node * a.ldy;
-        // leaves are not read again by this kernel: stream them past L2
-        const bool stream_y = hints && nodew >= 0;
+        // leaves are not read again by this kernel: stream them past L2 (not
+        // in a first pass, whose rows the second pass reads back)
+        const bool stream_y = hints && nodew >= 0 && !a.skip_parent;
 #pragma unroll
         for (int v = 0; v < VPL; ++v) {
           const int vi = tl + v * TL;
@@ -1245,7 +1341,7 @@ __global__ void __launch_bounds__(BLOCK) fwd_stream_kernel(const FwdArgs a, cons
               store_vec<YT, V>(yrow + (int64_t)vi * V, acc[v]);
           }
         }
-        if (nodew < 0) {
+        if (nodew < 0 && !a.skip_parent) {
           if constexpr (sizeof(YT) != 4) {
             float* srow = a.pstate + (int64_t)ss * a.ldp;
 #pragma unroll
@@ -1281,7 +1377,7 @@ __global__ void __launch_bounds__(BLOCK) fwd_stream_kernel(const FwdArgs a, cons
       }
     }
   }
-  finish_block(a.qs, epoch);
+  finish_block(a.qs, epoch, a.publish_epoch != 0);
 }
 
 // ============================================================================

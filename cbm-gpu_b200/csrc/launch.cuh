@@ -152,6 +152,17 @@ int launch_tr_t(cbm_plan* P, const TrArgs& a, cudaStream_t st) {
   return cuda_status(cudaGetLastError());
 }
 
+template <int VPL, int V>
+int launch_prop_t(cbm_plan* P, const PropArgs& a, cudaStream_t st) {
+  static GridCache cache;
+  auto kern = prop_kernel<VPL, V>;
+  const int grid = cached_grid(cache, kern, P->device, kThreads, 0);
+  if (grid <= 0) return CBM_ERR_CUDA;
+  kern<<<grid, kThreads, 0, st>>>(a);
+  P->launches++;
+  return cuda_status(cudaGetLastError());
+}
+
 // ---- per-unit entry points (launch_*.cu) ------------------------------------------
 int launch_staged_f32(cbm_plan* P, const FwdArgs& a, int team, int vpl, cudaStream_t st);
 int launch_staged_bf16_f32(cbm_plan* P, const FwdArgs& a, int team, int vpl, cudaStream_t st);
@@ -162,6 +173,8 @@ int launch_fwd_f32(cbm_plan* P, const FwdArgs& a, bool vec, int vpl, cudaStream_
 int launch_fwd_bf16(cbm_plan* P, const FwdArgs& a, int32_t ydt, bool vec, int vpl, cudaStream_t st);
 // compensated propagation: BF16 X only (the precision form), register kernel
 int launch_fwd_comp(cbm_plan* P, const FwdArgs& a, int32_t ydt, bool vec, int vpl, cudaStream_t st);
+// second pass of a two-pass product (FP32 Y)
+int launch_prop(cbm_plan* P, const PropArgs& a, bool vec, int vpl, cudaStream_t st);
 int launch_rev(cbm_plan* P, const RevArgs& a, int32_t gdt, bool vec, int vpl, cudaStream_t st);
 int launch_tr(cbm_plan* P, const TrArgs& a, int32_t gdt, int32_t ddt, bool vec, int vpl, cudaStream_t st);
 

@@ -1,5 +1,5 @@
-// Register-gather forward kernel instantiations: FP32 X, and the compensated
-// (precision-form) BF16 kernels.
+// Register-gather forward kernel instantiations: FP32 X, the compensated
+// (precision-form) BF16 kernels, and the second pass of two-pass products.
 #include "launch.cuh"
 
 namespace cbm {
@@ -14,5 +14,15 @@ int launch_fwd_comp(cbm_plan* P, const FwdArgs& a, int32_t ydt, bool vec, int vp
   }
   return vec ? launch_fwd_v<__nv_bfloat16, __nv_bfloat16, 8, true>(P, a, vpl, st)
              : launch_fwd_v<__nv_bfloat16, __nv_bfloat16, 1, true>(P, a, vpl, st);
+}
+
+int launch_prop(cbm_plan* P, const PropArgs& a, bool vec, int vpl, cudaStream_t st) {
+  if (!vec) return launch_prop_t<1, 1>(P, a, st);
+  switch (vpl) {
+    case 1: return launch_prop_t<1, 4>(P, a, st);
+    case 2: return launch_prop_t<2, 4>(P, a, st);
+    case 4: return launch_prop_t<4, 4>(P, a, st);
+    default: return launch_prop_t<8, 4>(P, a, st);
+  }
 }
 }  // namespace cbm

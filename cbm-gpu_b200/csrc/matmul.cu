@@ -326,6 +326,12 @@ int64_t cbm_plan_workspace_bytes(const cbm_plan* P, int32_t op, int64_t n_cols, 
   return align256(rows * ldp * 4) + 256;
 }
 
+int cbm_plan_set_passes(cbm_plan* P, int32_t passes) {
+  if (!P || passes < CBM_PASSES_AUTO || passes > CBM_PASSES_TWO) return CBM_ERR_INVALID;
+  P->passes = passes;
+  return CBM_OK;
+}
+
 int cbm_plan_set_timeout(cbm_plan* P, int64_t ns) {
   if (!P || ns <= 0) return CBM_ERR_INVALID;
   P->timeout_ns = ns;
@@ -456,6 +462,7 @@ int matmul_impl(cbm_plan* P, int32_t op, float gin_scale, const void* x, int32_t
     a.n_units = (int32_t)P->n_units;
     a.hints = P->hot_rows > 0 ? 1 : 0;
     a.timeout_ns = P->timeout_ns;
+    a.publish_epoch = 1;
     int s_team = 0, s_vpl = 0;
     // The GIN form runs on the register kernel (its self term and state rows
     // stay out of the staged kernel's registers).  So does AUTO on trees where
@@ -468,8 +475,23 @@ int matmul_impl(cbm_plan* P, int32_t op, float gin_scale, const void* x, int32_t
     // (rows of at most 512 bytes: the widths measured; wider rows keep the
     // staged kernel, whose ring carries more bytes in flight per lane)
     const bool deep_tree = (P->n_items - P->n_root) * 2 > P->n_items && cols * elem_size(xdt) <= 512;
+    // Two passes (FP32 Y, no GIN term, no compensation): every row's delta sum
+    // first, with no parent waits, then the parent terms in level order
+    // (prop_kernel).  AUTO takes them on trees where most rows hang below
+    // level 0, the ones whose single pass is a chain of waits.
+    const bool two_pass = ydt == CBM_F32 && !gin && !comp && P->n_items > P->n_root &&
+                          (P->passes == CBM_PASSES_TWO ||
+                           (P->passes == CBM_PASSES_AUTO && (P->n_items - P->n_root) * 2 > P->n_items));
+    if (two_pass) {
+      // the first pass waits on nothing: level-0 claim sizes for every row
+      a.skip_parent = 1;
+      a.publish_epoch = 0;
+      a.n_root = a.n_items;
+      a.unit = nullptr;
+      a.n_units = 0;
+    }
     const bool staged = sh.vec && !gin && P->variant != CBM_VARIANT_REGISTER &&
-                        !(P->variant == CBM_VARIANT_AUTO && deep_tree) &&
+                        !(P->variant == CBM_VARIANT_AUTO && deep_tree && !two_pass) &&
                         staged_shape(nvec, sh.v, P->staged_team, &s_team, &s_vpl);
     const bool tma = staged && P->variant == CBM_VARIANT_TMA && tma_shape(nvec, sh.v, s_team, s_vpl);
     int rc;
@@ -487,10 +509,35 @@ int matmul_impl(cbm_plan* P, int32_t op, float gin_scale, const void* x, int32_t
     } else {
       // on such trees level-0 claims of two rows also serve narrow operands
       // better (40 BF16 columns on the GCN graph: 0.26 -> 0.17 ms)
-      if (P->variant == CBM_VARIANT_AUTO && deep_tree) a.rows_per_claim = std::min<int32_t>(a.rows_per_claim, 2);
+      if (P->variant == CBM_VARIANT_AUTO && deep_tree && !two_pass)
+        a.rows_per_claim = std::min<int32_t>(a.rows_per_claim, 2);
       rc = launch_fwd(P, a, xdt, ydt, sh.vec, vpl, st);
     }
     if (rc) return rc;
+    if (two_pass) {
+      PropArgs pa;
+      std::memset(&pa, 0, sizeof(pa));
+      pa.n_items = (int32_t)P->n_items;
+      pa.n_root = (int32_t)P->n_root;
+      pa.node = P->d_node;
+      pa.par = P->d_par;
+      pa.par_item = P->d_par_item;
+      pa.y = static_cast<float*>(a.y);
+      pa.ldy = ldy;
+      pa.mult = P->d_mult;
+      pa.prop_mode = prop;
+      pa.node_flag = P->d_node_flag;
+      pa.qs = P->d_qs;
+      pa.timeout_ns = P->timeout_ns;
+      // FP32 rows in 16-byte vectors where Y allows them
+      const bool yvec = cols % 4 == 0 && reinterpret_cast<uintptr_t>(a.y) % 16 == 0 && (ldy * 4) % 16 == 0;
+      const int64_t ynvec = yvec ? cols / 4 : cols;
+      int pteam, pvpl;
+      team_for(ynvec, &pteam, &pvpl);
+      pa.nvec = (int32_t)ynvec;
+      pa.team = pteam;
+      if ((rc = launch_prop(P, pa, yvec, pvpl, st))) return rc;
+    }
   }
   return CBM_OK;
 }

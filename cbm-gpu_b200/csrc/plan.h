@@ -31,6 +31,7 @@ struct cbm_plan {
   int32_t variant = 0;          // CBM_VARIANT_*: forward kernel choice
   int64_t hot_rows = 65536;     // columns whose X rows the staged kernel asks L2 to keep (0: no hints)
   int32_t staged_team = 0;      // lanes per team of the staged kernel (0: its default)
+  int32_t passes = 0;           // CBM_PASSES_*: fused product or delta pass + propagation pass
   int64_t launches = 0;
   int64_t last_grid = 0;
   long long timeout_ns = 1000000000ll;  // bounded waits: 1 s

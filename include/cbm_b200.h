@@ -173,6 +173,15 @@ enum {
 int cbm_plan_tune(cbm_plan* plan, int32_t chunk_nnz, int32_t rows_per_claim, int32_t rows_per_claim_deep,
                   int32_t variant, int64_t hot_rows, int32_t team, void* stream);
 
+/* How a product is executed (FP32 Y without the GIN term or compensation;
+ * other products always run fused).  FUSED: one pass, each row adds its
+ * parent's row as soon as it is final.  TWO: a first pass stores every row's
+ * delta sum without waiting on parents, a second adds the parent terms in
+ * tree-level order; same arithmetic, bit-identical results.  AUTO (default):
+ * two passes on trees where more than half of the rows hang below level 0. */
+enum { CBM_PASSES_AUTO = 0, CBM_PASSES_FUSED = 1, CBM_PASSES_TWO = 2 };
+int cbm_plan_set_passes(cbm_plan* plan, int32_t passes);
+
 /* Device scratch bytes a call with these operand types needs (0 is possible). */
 int64_t cbm_plan_workspace_bytes(const cbm_plan* plan, int32_t op, int64_t n_cols, int32_t x_dtype,
                                  int32_t y_dtype, int32_t adjoint);

@@ -70,11 +70,13 @@ GRAPHS = {
 @pytest.mark.parametrize("op", ["ax", "adx", "dadx"])
 @pytest.mark.parametrize("cols", [64, 256])
 @pytest.mark.parametrize("variant", ["register", "staged"])
-def test_forward_bit_exact_vs_oracle(graph, op, cols, variant):
+@pytest.mark.parametrize("passes", ["fused", "two"])
+def test_forward_bit_exact_vs_oracle(graph, op, cols, variant, passes):
     dev = _dev()
     ei, n = GRAPHS[graph]()
     a = _make(op, ei, alpha=0)
     a.plan.tune(variant=variant, rows_per_claim=5)
+    a.plan.set_passes(passes)
     assert a.plan.stat(7) == 0, "no row should be split at these sizes"
     g = torch.Generator(device="cpu").manual_seed(0)
     x = (torch.rand(n, cols, generator=g) * 2 - 1).to(dev)
@@ -146,12 +148,14 @@ def _abs_sum(op, a, x):
 
 
 @pytest.mark.parametrize("variant", ["register", "staged"])
-def test_deep_chain(variant):
+@pytest.mark.parametrize("passes", ["auto", "fused", "two"])
+def test_deep_chain(variant, passes):
     """A 600-deep chain: every row waits on its parent."""
     dev = _dev()
     ei, n = chain_graph(600)
     a = _make("ax", ei)
     a.plan.tune(variant=variant)
+    a.plan.set_passes(passes)
     assert a.plan.stats["levels"] == 600
     x = torch.randn(n, 32, device=dev)
     y = torch.empty_like(x)
@@ -356,3 +360,28 @@ def test_tma_gather_variant_bit_exact(cols, dtype, op):
         a.matmul(x, y)
         a.plan.check_device()
         np.testing.assert_array_equal(y.cpu().numpy(), _oracle(op, a, x))
+
+
+@pytest.mark.parametrize("op", ["ax", "adx", "dadx"])
+@pytest.mark.parametrize("cols", [40, 128])
+def test_two_pass_equals_fused_on_a_deep_tree(op, cols):
+    """On a tree where most rows hang below level 0 (where AUTO takes two
+    passes), the two-pass product equals the fused one and the oracle bit for
+    bit, for BF16 X too (FP32 Y)."""
+    dev = _dev()
+    ei = near_dup_graph(6000, seed=41, frac=0.8, flip=0.05, deg=10)
+    a = _make(op, ei, alpha=0)
+    st = a.plan.stats
+    assert st["levels"] >= 3 and st["chunks"] == 0
+    for xdt in (torch.float32, torch.bfloat16):
+        x = torch.randn(6000, cols, device=dev).to(xdt)
+        ys = {}
+        for passes in ("fused", "two", "auto"):
+            a.plan.set_passes(passes)
+            y = torch.full((6000, cols), float("nan"), device=dev)
+            a.matmul(x, y)
+            ys[passes] = y.cpu().numpy()
+        assert np.array_equal(ys["two"], ys["fused"])
+        assert np.array_equal(ys["auto"], ys["fused"])
+        np.testing.assert_array_equal(ys["two"], _oracle(op, a, x.float()))
+    a.plan.check_device()
