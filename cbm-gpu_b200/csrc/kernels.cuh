@@ -634,9 +634,11 @@ __global__ void __launch_bounds__(kThreads) prop_kernel(const PropArgs a) {
         const float dp = ratio ? __ldg(a.mult + p) : 1.f;
         const float* yp_row = a.y + (int64_t)p * a.ldy;
         float* yv_row = a.y + (int64_t)node * a.ldy;
+        // passes of TL * VPL vectors cover rows of any width
+        for (int vb = 0; vb < a.nvec; vb += TL * VPL) {
 #pragma unroll
         for (int v = 0; v < VPL; ++v) {
-          const int vi = tl + v * TL;
+          const int vi = vb + tl + v * TL;
           if (vi < a.nvec) {
             float yp[V], yv[V];
             load_f32_cg<V>(yp_row + vi * V, yp);
@@ -650,6 +652,7 @@ __global__ void __launch_bounds__(kThreads) prop_kernel(const PropArgs a) {
             }
             store_f32<V>(yv_row + vi * V, yv);
           }
+        }
         }
       }
       if (nodew < 0) {

@@ -17,7 +17,7 @@ int launch_fwd_comp(cbm_plan* P, const FwdArgs& a, int32_t ydt, bool vec, int vp
 }
 
 int launch_prop(cbm_plan* P, const PropArgs& a, bool vec, int vpl, cudaStream_t st) {
-  if (!vec) return launch_prop_t<1, 1>(P, a, st);
+  if (!vec) return vpl <= 1 ? launch_prop_t<1, 1>(P, a, st) : launch_prop_t<4, 1>(P, a, st);
   switch (vpl) {
     case 1: return launch_prop_t<1, 4>(P, a, st);
     case 2: return launch_prop_t<2, 4>(P, a, st);

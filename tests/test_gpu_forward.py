@@ -301,25 +301,45 @@ def test_repeatable_and_graph_capturable():
     a.plan.check_device()
 
 
-def test_bounded_wait_times_out_and_recovers():
+@pytest.mark.parametrize("passes", ["fused", "two"])
+def test_bounded_wait_times_out_and_recovers(passes):
     """A row made to wait on a flag that nothing sets: the kernel returns, the
-    status says timeout, and the plan keeps working."""
+    status says timeout, and the plan keeps working.  Fused: a level-0 item
+    given a leaf as its parent.  Two passes: the deepest item given a leaf
+    below level 0 as its parent (the propagation pass waits on such parents)."""
     dev = _dev()
     from cbm import _lib
 
-    a = _make("ax", near_dup_graph(500, seed=4))
+    n = 500
+    a = _make("ax", near_dup_graph(n, seed=4))
     p = a.plan
+    p.set_passes(passes)
+    par = np.asarray(a.parent)
+    depth = np.zeros(n, np.int64)
+    for v in range(n):
+        u = v
+        while par[u] != n:
+            u = par[u]
+            depth[v] += 1
+    order = np.argsort(depth, kind="stable")  # the plan's item order: by level, stable by node id
     has_child = set(a.mca_src_idx.cpu().tolist())
-    leaf = next(v for v in range(500) if v not in has_child)
+    if passes == "fused":
+        item = 0
+        leaf = next(v for v in range(n) if v not in has_child)
+    else:
+        item = n - 1
+        leaf = next(int(v) for v in order[::-1] if depth[v] > 0 and int(v) not in has_child and v != order[item])
     p.set_timeout(5_000_000)  # 5 ms
-    rc = p._lib.cbm_plan_debug_set_parent(p._h, 0, leaf, None)
+    rc = p._lib.cbm_plan_debug_set_parent(p._h, item, leaf, None)
     assert rc == 0
-    x = torch.randn(500, 32, device=dev)
+    x = torch.randn(n, 32, device=dev)
     y = torch.empty_like(x)
     a.matmul(x, y)
     st, info = p.error()
     assert st == _lib.ERR_TIMEOUT
-    assert p._lib.cbm_plan_debug_set_parent(p._h, 0, -1, None) == 0
+    # restore the item's own parent
+    own = int(par[order[item]])
+    assert p._lib.cbm_plan_debug_set_parent(p._h, item, -1 if own == n else own, None) == 0
     p.set_timeout(1_000_000_000)
     a.matmul(x, y)
     assert p.error()[0] == _lib.OK
