@@ -364,7 +364,7 @@ def gcn_timing(steps, warmup):
         hw = torch.randn(n, 40, device="cuda", generator=g).to(dt)
         y40 = torch.empty(n, 40, device="cuda")
         g40 = torch.randn(n, 40, device="cuda", generator=g)
-        dx40 = torch.empty(n, 40, dtype=dt, device="cuda")
+        dx40 = torch.empty(n, 40, device="cuda")  # FP32 gradient in, FP32 out (as autograd runs it)
 
         def cbm_work():
             a.matmul(x_act, y128)

@@ -477,16 +477,12 @@ int matmul_impl(cbm_plan* P, int32_t op, float gin_scale, const void* x, int32_t
     const bool deep_tree = (P->n_items - P->n_root) * 2 > P->n_items && cols * elem_size(xdt) <= 512;
     // Two passes (FP32 Y, no GIN term, no compensation): every row's delta sum
     // first, with no parent waits, then the parent terms in level order
-    // (prop_kernel).  AUTO takes them only on trees of kTwoPassLevels levels
-    // or more where most rows hang below level 0: long chains, where the
-    // fused pass serialises a gather per level.  On shallow deep-ish trees the
-    // fused pass measured faster (the 7-level GCN graph, 40 FP32 columns:
-    // 179 us fused, 259 us in two passes).
-    constexpr int64_t kTwoPassLevels = 64;
+    // (prop_kernel).  Opt-in: AUTO keeps the fused pass, which measured as
+    // fast or faster on every tree tried (the 7-level GCN graph, 40 FP32
+    // columns: 179 us fused, 259 us in two passes; a 2,000-deep chain: 4.1 ms
+    // either way).
     const bool two_pass = ydt == CBM_F32 && !gin && !comp && P->n_items > P->n_root &&
-                          (P->passes == CBM_PASSES_TWO ||
-                           (P->passes == CBM_PASSES_AUTO && P->levels >= kTwoPassLevels &&
-                            (P->n_items - P->n_root) * 2 > P->n_items));
+                          P->passes == CBM_PASSES_TWO;
     if (two_pass) {
       // the first pass waits on nothing: level-0 claim sizes for every row
       a.skip_parent = 1;
