@@ -25,7 +25,7 @@ BUILD_EXHAUSTIVE = 1
 COALESCE_SYMMETRIZE, COALESCE_DROP_SELF = 1, 2
 S_DELTA_ROW, S_DELTA_COL, S_DELTA_VAL, S_BRANCHES, S_SRC, S_DST, S_PARENT, S_CSR_PTR, S_CSR_COL, \
     S_CSR_VAL = range(10)
-S_N_CANDIDATES, S_TREE_COST, S_NNZ_A = 100, 101, 102
+S_N_CANDIDATES, S_TREE_COST, S_NNZ_A, S_SYMMETRIC = 100, 101, 102, 103
 P_ROWS, P_COLS, P_NNZ, P_EDGES, P_BRANCHES, P_LEVELS, P_INTERNAL, P_CHUNKS, P_LONG_ROWS, P_UNIT_VALUES, \
     P_GRID, P_LAUNCHES = range(12)
 

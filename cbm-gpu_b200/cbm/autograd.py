@@ -4,7 +4,10 @@
 cbm4mm / cbm4ad / cbm4dad instance; its backward computes A_op^T g in CBM
 form: a reverse tree propagation (children summed into parents, deepest level
 first) followed by a gather over the transposed delta matrix, both on the GPU
-(cbm_matmul_adjoint).  No dense or torch.sparse matrix is formed.
+(cbm_matmul_adjoint).  Where the operator equals its transpose (a symmetric
+A, as the undirected graphs of a GCN give, with A or D^-1/2 A D^-1/2), the
+backward is the forward product itself: A^T g = A g, and the forward kernel
+is the faster of the two.  No dense or torch.sparse matrix is formed.
 """
 from __future__ import annotations
 
@@ -36,7 +39,10 @@ class CBMProduct(torch.autograd.Function):
         want = ctx.x_dtype
         ddt = want if (gdt, want) in _PAIRS else torch.float32
         dx = torch.empty(op.plan.n_cols, g.shape[1], dtype=ddt, device=g.device)
-        op.adjoint(g, dx)
+        if getattr(op, "self_adjoint", False):
+            op.matmul(g, dx)
+        else:
+            op.adjoint(g, dx)
         return dx.to(want), None, None
 
 

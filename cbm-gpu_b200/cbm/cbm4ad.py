@@ -18,6 +18,7 @@ __all__ = ["cbm4ad"]
 
 class cbm4ad(cbm4mm):  # noqa: N801
     _op = "adx"
+    _transpose_free_if_symmetric = False  # (A D^-1/2)^T = D^-1/2 A^T
 
     def __init__(self, edge_index, edge_values, alpha=0, cache_dir=None, cluster=None):
         super().__init__(edge_index, edge_values, alpha, cache_dir, cluster)

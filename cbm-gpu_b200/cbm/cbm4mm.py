@@ -22,6 +22,8 @@ __all__ = ["cbm4mm"]
 
 class cbm4mm:  # noqa: N801 (the reference's class name)
     _op = "ax"
+    # the operator equals its transpose when A does (A, D^-1/2 A D^-1/2; not A D^-1/2)
+    _transpose_free_if_symmetric = True
 
     def __init__(self, edge_index, edge_values, alpha=0, cache_dir=None, cluster=None):
         """Additions to the reference's arguments: cache_dir reuses the
@@ -45,6 +47,7 @@ class cbm4mm:  # noqa: N801 (the reference's class name)
         self.mca_src_idx = torch.from_numpy(s.src).to(dtype=torch.int32, device="cuda")
         self.mca_dst_idx = torch.from_numpy(s.dst).to(dtype=torch.int32, device="cuda")
         self.parent = s.parent  # host int32 [N], N = virtual root
+        self.symmetric = bool(s.symmetric)  # A == A^T (found by the constructor)
         self._plan = Plan(s.csr_ptr, s.csr_col, s.csr_val, num_rows, num_rows, s.branches, s.src, s.dst,
                           host=True)
         self.cusparse_extension = cusparseCBM._from_plan(self._plan, "ax", None, False)
@@ -68,8 +71,15 @@ class cbm4mm:  # noqa: N801 (the reference's class name)
         the current stream: synchronise it before reading y."""
         self._plan.matmul_host(self._op, x, y, slab_cols)
 
+    @property
+    def self_adjoint(self):
+        """True when this operator equals its transpose (A symmetric, and the
+        operator A or D^-1/2 A D^-1/2): then A^T g = A g."""
+        return self.symmetric and self._transpose_free_if_symmetric
+
     def adjoint(self, g, dx):
-        """dx <- (this operator)^T g."""
+        """dx <- (this operator)^T g, by the adjoint kernels (reverse tree
+        propagation, then the transposed-delta gather)."""
         self._plan.adjoint(self._op, g, dx)
 
     def forward(self, x, out_dtype=None):

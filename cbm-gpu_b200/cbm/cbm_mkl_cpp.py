@@ -48,7 +48,7 @@ __all__ = ["init", "build", "build_cached", "save_structure", "load_structure", 
            "s_fused_update_csr_int32", "device_status", "check_device"]
 
 # on-disk format: an .npz of every Structure array plus these scalars
-_FORMAT = "cbm-structure-1"
+_FORMAT = "cbm-structure-2"
 
 
 @dataclass
@@ -69,6 +69,7 @@ class Structure:
     n_candidates: int
     tree_cost: int
     nnz_a: int
+    symmetric: bool = False  # A == A^T
 
 
 _FIELDS = [
@@ -131,6 +132,7 @@ def build(row, col, n_rows, alpha=0, n_threads=0, exhaustive=False, cluster=None
             n_candidates=int(lib.cbm_structure_len(h, _lib.S_N_CANDIDATES)),
             tree_cost=int(lib.cbm_structure_len(h, _lib.S_TREE_COST)),
             nnz_a=int(lib.cbm_structure_len(h, _lib.S_NNZ_A)),
+            symmetric=bool(lib.cbm_structure_len(h, _lib.S_SYMMETRIC)),
             **out,
         )
     finally:
@@ -155,7 +157,7 @@ def save_structure(path, s, key=""):
     import os
 
     arrays = {name: getattr(s, name) for name, _, _ in _FIELDS}
-    meta = np.array([s.n, s.n_candidates, s.tree_cost, s.nnz_a], dtype=np.int64)
+    meta = np.array([s.n, s.n_candidates, s.tree_cost, s.nnz_a, int(s.symmetric)], dtype=np.int64)
     tmp = f"{path}.tmp{os.getpid()}"
     with open(tmp, "wb") as f:
         np.savez(f, _format=np.array(_FORMAT), _key=np.array(key), _meta=meta, **arrays)
@@ -172,9 +174,9 @@ def load_structure(path, key=None):
     with np.load(path) as d:
         if str(d["_format"]) != _FORMAT or (key is not None and str(d["_key"]) != key):
             return None
-        n, cand, cost, nnz_a = (int(v) for v in d["_meta"])
+        n, cand, cost, nnz_a, sym = (int(v) for v in d["_meta"])
         arrays = {name: d[name] for name, _, _ in _FIELDS}
-    return Structure(n=n, n_candidates=cand, tree_cost=cost, nnz_a=nnz_a, **arrays)
+    return Structure(n=n, n_candidates=cand, tree_cost=cost, nnz_a=nnz_a, symmetric=bool(sym), **arrays)
 
 
 def structure_key(row, col, n_rows, alpha, cluster=None):

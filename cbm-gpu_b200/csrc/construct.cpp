@@ -531,10 +531,27 @@ struct cbm_structure {
   int64_t n_candidates = 0;     // tree candidates (without the N virtual edges)
   int64_t tree_cost = 0;        // total weight of the chosen arborescence
   int64_t nnz_a = 0;            // nnz of the coalesced A
+  bool symmetric = false;       // A == A^T
   std::string error;
 };
 
 namespace {
+
+// A == A^T: every (i, j) has (j, i), found by binary search in row j's sorted
+// columns (rows in parallel).
+bool is_symmetric(const Csr& a) {
+  bool sym = true;
+#pragma omp parallel for reduction(&& : sym) schedule(dynamic, 4096)
+  for (int64_t i = 0; i < a.n; ++i) {
+    for (int64_t k = a.ptr[i]; k < a.ptr[i + 1] && sym; ++k) {
+      const int32_t j = a.idx[k];
+      const int32_t* b = a.idx.data() + a.ptr[j];
+      const int32_t* e = a.idx.data() + a.ptr[j + 1];
+      if (!std::binary_search(b, e, (int32_t)i)) sym = false;
+    }
+  }
+  return sym;
+}
 
 // Entries of A[v] - A[u] (u = -1: A[v] as +1 entries) in increasing column
 // order, written at out (when not null); returns their number.
@@ -654,6 +671,7 @@ int cbm_build_clustered(const int32_t* row, const int32_t* col, int64_t nnz, int
     const int64_t n = n_rows;
     Csr a = coo_to_csr(row, col, nnz, n);
     s->nnz_a = (int64_t)a.idx.size();
+    s->symmetric = is_symmetric(a);
     std::vector<Pair> pairs = (flags & CBM_BUILD_EXHAUSTIVE) ? candidate_pairs_exhaustive(a, alpha, n_threads)
                                                               : candidate_pairs(a, alpha, n_threads);
     // clustered: a row's parent may only be a row of its own cluster (the
@@ -801,6 +819,7 @@ int64_t cbm_structure_len(const cbm_structure* s, int32_t which) {
     case CBM_S_N_CANDIDATES: return s->n_candidates;
     case CBM_S_TREE_COST: return s->tree_cost;
     case CBM_S_NNZ_A: return s->nnz_a;
+    case CBM_S_SYMMETRIC: return s->symmetric ? 1 : 0;
     default: return -1;
   }
 }

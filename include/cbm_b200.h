@@ -112,7 +112,8 @@ enum {
   CBM_S_CSR_VAL = 9,   /* float [Z]                                           */
   CBM_S_N_CANDIDATES = 100, /* length-only queries */
   CBM_S_TREE_COST = 101,
-  CBM_S_NNZ_A = 102
+  CBM_S_NNZ_A = 102,
+  CBM_S_SYMMETRIC = 103     /* 1 if A == A^T (then A^T G = A G) */
 };
 int64_t cbm_structure_len(const cbm_structure* s, int32_t which);
 int cbm_structure_copy(const cbm_structure* s, int32_t which, void* dst);

@@ -208,3 +208,33 @@ def test_transposed_index_sorted_on_device_equals_host_counting_sort(graph):
     ref = _adj_f64("ax", ei, a.num_nodes, g)
     assert np.abs(d1.cpu().numpy() - ref).max() <= 1e-4 * max(1.0, np.abs(ref).max())
     p.check_device()
+
+
+def test_backward_of_a_self_adjoint_operator_is_its_forward():
+    """A symmetric A: cbm4mm and cbm4dad are their own transposes, so autograd's
+    backward runs the forward product (bit-identical to matmul on g) and still
+    matches the adjoint kernels and FP64; cbm4ad (A D^-1/2) is not, and on a
+    directed graph nothing is."""
+    from cbm import cbm_mkl_cpp
+
+    dev = torch.device("cuda")
+    n = 2500
+    ei = near_dup_graph(n, seed=33)
+    assert cbm_mkl_cpp.build(ei[0], ei[1], n, 0).symmetric
+    for op in ("ax", "dadx", "adx"):
+        a = _make(op, ei)
+        assert a.self_adjoint == (op != "adx")
+        x = torch.randn(n, 24, device=dev, requires_grad=True)
+        w = torch.randn(n, 24, device=dev)
+        (a.forward(x) * w).sum().backward()
+        via_kernels = torch.empty(n, 24, device=dev)
+        a.adjoint(w, via_kernels)
+        torch.testing.assert_close(x.grad, via_kernels, rtol=1e-5, atol=1e-5)
+        if a.self_adjoint:
+            fwd = torch.empty(n, 24, device=dev)
+            a.matmul(w, fwd)
+            assert torch.equal(x.grad, fwd)
+        a.plan.check_device()
+    directed = random_graph(1500, 8, seed=9, symmetric=False)
+    d = _make("ax", directed)
+    assert not d.symmetric and not d.self_adjoint
