@@ -278,14 +278,15 @@ __host__ __device__ constexpr int unroll_for() {
   return (32 / (VPL * V)) < 1 ? 1 : ((32 / (VPL * V)) > 8 ? 8 : (32 / (VPL * V)));
 }
 
-// acc += sum over entries [beg, end) of scale_k * X[col_k]
-template <typename XT, int VPL, int V>
+// acc += sum over entries [beg, end) of scale_k * X[col_k], UF entries' gathers
+// in flight per lane (0: unroll_for's choice)
+template <typename XT, int VPL, int V, int UF = 0>
 __device__ __forceinline__ void gather_range(float (&acc)[VPL][V], const XT* __restrict__ x, int64_t ldx, int nvec,
                                              const uint32_t* __restrict__ ent, const float* __restrict__ val,
                                              int64_t beg, int64_t end, int scale_mode,
                                              const float* __restrict__ mult, float dv, int tl, int TL,
                                              unsigned tmask) {
-  constexpr int U = unroll_for<VPL, V>();
+  constexpr int U = UF > 0 ? UF : unroll_for<VPL, V>();
   for (int64_t base = beg; base < end; base += TL) {
     const int64_t idx = base + tl;
     uint32_t e = 0;
@@ -337,7 +338,19 @@ __device__ __forceinline__ void gather_range(float (&acc)[VPL][V], const XT* __r
   }
 }
 
-template <typename XT, typename YT, int VPL, int V>
+// Rows of one 16-byte vector per lane, where products are latency-bound
+// (the 170K-node GCN graph, L2-resident): with X and Y of one type (and no
+// compensation) four blocks of 256 threads per SM (at most 64 registers) and
+// two gathers in flight per lane measured faster than three blocks with four
+// or eight in flight (128 BF16 columns 0.235 -> 0.210 ms, 128 FP32 0.311 ->
+// 0.258 ms, 40 FP32 0.180 -> 0.162 ms); the BF16-in, FP32-out kernel measured
+// slower that way (40 columns 0.164 -> 0.217 ms) and keeps the default.
+template <typename XT, typename YT, int VPL, bool COMP>
+__host__ __device__ constexpr bool fwd_narrow_occupancy() {
+  return VPL == 1 && sizeof(XT) == sizeof(YT) && !COMP;
+}
+
+template <typename XT, typename YT, int VPL, int V, bool COMP = false>
 __device__ __forceinline__ void fwd_chunk(const FwdArgs& a, int k, unsigned epoch, int tl, int TL, unsigned tmask) {
   float acc[VPL][V];
 #pragma unroll
@@ -347,8 +360,9 @@ __device__ __forceinline__ void fwd_chunk(const FwdArgs& a, int k, unsigned epoc
   const int item = a.chunk_item[k];
   const int node = a.node[item] & 0x7fffffff;
   const float dv = (a.scale_mode == SCALE_DCOL_DROW) ? __ldg(a.mult + node) : 1.f;
-  gather_range<XT, VPL, V>(acc, static_cast<const XT*>(a.x), a.ldx, a.nvec, a.cent, a.cval, a.chunk_beg[k],
-                           a.chunk_end[k], a.scale_mode, a.mult, dv, tl, TL, tmask);
+  gather_range<XT, VPL, V, fwd_narrow_occupancy<XT, YT, VPL, COMP>() ? 2 : 0>(
+      acc, static_cast<const XT*>(a.x), a.ldx, a.nvec, a.cent, a.cval, a.chunk_beg[k], a.chunk_end[k],
+      a.scale_mode, a.mult, dv, tl, TL, tmask);
   float* prow = a.partial + (int64_t)k * a.ldp;
 #pragma unroll
   for (int v = 0; v < VPL; ++v) {
@@ -395,8 +409,9 @@ __device__ __forceinline__ void fwd_row(const FwdArgs& a, int item, unsigned epo
   const float dv = need_dv ? __ldg(a.mult + node) : 1.f;
   const int c0 = a.chunk0[item];
   if (c0 < 0) {
-    gather_range<XT, VPL, V>(acc, static_cast<const XT*>(a.x), a.ldx, a.nvec, a.ent, a.val, a.ptr[item],
-                             a.ptr[item + 1], a.scale_mode, a.mult, dv, tl, TL, tmask);
+    gather_range<XT, VPL, V, fwd_narrow_occupancy<XT, YT, VPL, COMP>() ? 2 : 0>(
+        acc, static_cast<const XT*>(a.x), a.ldx, a.nvec, a.ent, a.val, a.ptr[item], a.ptr[item + 1],
+        a.scale_mode, a.mult, dv, tl, TL, tmask);
   } else {
     for (int k = c0; k < a.n_chunks && a.chunk_item[k] == item; ++k) {
       if (!wait_flag(a.chunk_flag + k, epoch, a.qs, a.timeout_ns, (long long)k)) continue;
@@ -535,7 +550,8 @@ __device__ __forceinline__ void finish_block(QueueState* qs, unsigned epoch, boo
 }
 
 template <typename XT, typename YT, int VPL, int V, bool COMP = false>
-__global__ void __launch_bounds__(kThreads) fwd_kernel(const FwdArgs a) {
+__global__ void __launch_bounds__(kThreads, (fwd_narrow_occupancy<XT, YT, VPL, COMP>() ? 4 : 1))
+    fwd_kernel(const FwdArgs a) {
   const int lane = threadIdx.x & 31;
   const int TL = a.team;
   const int team = lane / TL;
@@ -551,7 +567,7 @@ __global__ void __launch_bounds__(kThreads) fwd_kernel(const FwdArgs a) {
       base = __shfl_sync(0xffffffffu, base, 0);
       if (base >= (unsigned)a.n_chunks) break;
       const unsigned k = base + team;
-      if (k < (unsigned)a.n_chunks) fwd_chunk<XT, YT, VPL, V>(a, (int)k, epoch, tl, TL, tmask);
+      if (k < (unsigned)a.n_chunks) fwd_chunk<XT, YT, VPL, V, COMP>(a, (int)k, epoch, tl, TL, tmask);
       __syncwarp();
     }
   }
