@@ -338,19 +338,28 @@ __device__ __forceinline__ void gather_range(float (&acc)[VPL][V], const XT* __r
   }
 }
 
-// Rows of one 16-byte vector per lane, where products are latency-bound
-// (the 170K-node GCN graph, L2-resident): with X and Y of one type (and no
-// compensation) four blocks of 256 threads per SM (at most 64 registers) and
-// two gathers in flight per lane measured faster than three blocks with four
-// or eight in flight (128 BF16 columns 0.235 -> 0.210 ms, 128 FP32 0.311 ->
-// 0.258 ms, 40 FP32 0.180 -> 0.162 ms); the BF16-in, FP32-out kernel measured
-// slower that way (40 columns 0.164 -> 0.217 ms) and keeps the default.
-template <typename XT, typename YT, int VPL, bool COMP>
-__host__ __device__ constexpr bool fwd_narrow_occupancy() {
-  return VPL == 1 && sizeof(XT) == sizeof(YT) && !COMP;
+// Resident blocks per SM of the register kernel.  Rows of one 16-byte vector
+// per lane are latency-bound where X is L2-resident, and more warps hide more
+// of the latency, at the cost of registers (gathers in flight).  Measured on
+// B200, bit-identical results either way:
+//   X and Y of one type: 4 blocks (at most 64 registers) with two gathers in
+//     flight per lane (170K-node GCN graph: 128 BF16 columns 0.235 -> 0.210
+//     ms, 128 FP32 0.311 -> 0.258, 40 FP32 0.180 -> 0.162);
+//   BF16 X, FP32 Y: 3 blocks (at most 85 registers) where most rows wait on a
+//     parent (GCN graph, 40 columns: 0.160 ms against 0.196 with 2 blocks and
+//     0.210 with 4); WIDE, taken on shallower trees: 4 blocks with two in
+//     flight (512-graph batch, 64 columns: 4.87 ms against 5.44 with 3 blocks
+//     and 7.53 with 2).
+template <typename XT, typename YT, int VPL, bool COMP, bool WIDE>
+__host__ __device__ constexpr int fwd_min_blocks() {
+  return (VPL != 1 || COMP) ? 1 : ((sizeof(XT) == sizeof(YT) || WIDE) ? 4 : 3);
+}
+template <typename XT, typename YT, int VPL, bool COMP, bool WIDE>
+__host__ __device__ constexpr int fwd_in_flight() {
+  return fwd_min_blocks<XT, YT, VPL, COMP, WIDE>() == 4 ? 2 : 0;  // 0: unroll_for's choice
 }
 
-template <typename XT, typename YT, int VPL, int V, bool COMP = false>
+template <typename XT, typename YT, int VPL, int V, bool COMP = false, bool WIDE = false>
 __device__ __forceinline__ void fwd_chunk(const FwdArgs& a, int k, unsigned epoch, int tl, int TL, unsigned tmask) {
   float acc[VPL][V];
 #pragma unroll
@@ -360,7 +369,7 @@ __device__ __forceinline__ void fwd_chunk(const FwdArgs& a, int k, unsigned epoc
   const int item = a.chunk_item[k];
   const int node = a.node[item] & 0x7fffffff;
   const float dv = (a.scale_mode == SCALE_DCOL_DROW) ? __ldg(a.mult + node) : 1.f;
-  gather_range<XT, VPL, V, fwd_narrow_occupancy<XT, YT, VPL, COMP>() ? 2 : 0>(
+  gather_range<XT, VPL, V, fwd_in_flight<XT, YT, VPL, COMP, WIDE>()>(
       acc, static_cast<const XT*>(a.x), a.ldx, a.nvec, a.cent, a.cval, a.chunk_beg[k], a.chunk_end[k],
       a.scale_mode, a.mult, dv, tl, TL, tmask);
   float* prow = a.partial + (int64_t)k * a.ldp;
@@ -395,7 +404,7 @@ __device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
   e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bp)), __fsub_rn(b, bp));
 }
 
-template <typename XT, typename YT, int VPL, int V, bool COMP = false>
+template <typename XT, typename YT, int VPL, int V, bool COMP = false, bool WIDE = false>
 __device__ __forceinline__ void fwd_row(const FwdArgs& a, int item, unsigned epoch, int tl, int TL, unsigned tmask) {
   float acc[VPL][V];
 #pragma unroll
@@ -409,7 +418,7 @@ __device__ __forceinline__ void fwd_row(const FwdArgs& a, int item, unsigned epo
   const float dv = need_dv ? __ldg(a.mult + node) : 1.f;
   const int c0 = a.chunk0[item];
   if (c0 < 0) {
-    gather_range<XT, VPL, V, fwd_narrow_occupancy<XT, YT, VPL, COMP>() ? 2 : 0>(
+    gather_range<XT, VPL, V, fwd_in_flight<XT, YT, VPL, COMP, WIDE>()>(
         acc, static_cast<const XT*>(a.x), a.ldx, a.nvec, a.ent, a.val, a.ptr[item], a.ptr[item + 1],
         a.scale_mode, a.mult, dv, tl, TL, tmask);
   } else {
@@ -549,8 +558,8 @@ __device__ __forceinline__ void finish_block(QueueState* qs, unsigned epoch, boo
   }
 }
 
-template <typename XT, typename YT, int VPL, int V, bool COMP = false>
-__global__ void __launch_bounds__(kThreads, (fwd_narrow_occupancy<XT, YT, VPL, COMP>() ? 4 : 1))
+template <typename XT, typename YT, int VPL, int V, bool COMP = false, bool WIDE = false>
+__global__ void __launch_bounds__(kThreads, (fwd_min_blocks<XT, YT, VPL, COMP, WIDE>()))
     fwd_kernel(const FwdArgs a) {
   const int lane = threadIdx.x & 31;
   const int TL = a.team;
@@ -567,7 +576,7 @@ __global__ void __launch_bounds__(kThreads, (fwd_narrow_occupancy<XT, YT, VPL, C
       base = __shfl_sync(0xffffffffu, base, 0);
       if (base >= (unsigned)a.n_chunks) break;
       const unsigned k = base + team;
-      if (k < (unsigned)a.n_chunks) fwd_chunk<XT, YT, VPL, V, COMP>(a, (int)k, epoch, tl, TL, tmask);
+      if (k < (unsigned)a.n_chunks) fwd_chunk<XT, YT, VPL, V, COMP, WIDE>(a, (int)k, epoch, tl, TL, tmask);
       __syncwarp();
     }
   }
@@ -584,7 +593,7 @@ __global__ void __launch_bounds__(kThreads, (fwd_narrow_occupancy<XT, YT, VPL, C
     for (int r = 0; r < R; ++r) {
       const unsigned item = base + team + (unsigned)(r * teams);
       if (item >= (unsigned)a.n_items) break;
-      fwd_row<XT, YT, VPL, V, COMP>(a, (int)item, epoch, tl, TL, tmask);
+      fwd_row<XT, YT, VPL, V, COMP, WIDE>(a, (int)item, epoch, tl, TL, tmask);
     }
     __syncwarp();
   }

@@ -43,10 +43,10 @@ int cached_grid(GridCache& c, K kernel, int device, int block, int smem) {
   return g;
 }
 
-template <typename XT, typename YT, int VPL, int V, bool COMP = false>
+template <typename XT, typename YT, int VPL, int V, bool COMP = false, bool WIDE = false>
 int launch_fwd_t(cbm_plan* P, const FwdArgs& a, cudaStream_t st) {
   static GridCache cache;
-  auto kern = fwd_kernel<XT, YT, VPL, V, COMP>;
+  auto kern = fwd_kernel<XT, YT, VPL, V, COMP, WIDE>;
   const int grid = cached_grid(cache, kern, P->device, kThreads, 0);
   if (grid <= 0) return CBM_ERR_CUDA;
   kern<<<grid, kThreads, 0, st>>>(a);
@@ -170,7 +170,9 @@ int launch_staged_bf16_bf16(cbm_plan* P, const FwdArgs& a, int team, int vpl, cu
 int launch_tma(cbm_plan* P, const FwdArgs& a, int32_t xdt, int32_t ydt, int team, int vpl, const CUtensorMap& map,
                cudaStream_t st);
 int launch_fwd_f32(cbm_plan* P, const FwdArgs& a, bool vec, int vpl, cudaStream_t st);
-int launch_fwd_bf16(cbm_plan* P, const FwdArgs& a, int32_t ydt, bool vec, int vpl, cudaStream_t st);
+// wide: on trees where few rows wait on a parent, one-vector rows of BF16 X
+// and FP32 Y take the 4-block instantiation (fwd_min_blocks)
+int launch_fwd_bf16(cbm_plan* P, const FwdArgs& a, int32_t ydt, bool vec, int vpl, bool wide, cudaStream_t st);
 // compensated propagation: BF16 X only (the precision form), register kernel
 int launch_fwd_comp(cbm_plan* P, const FwdArgs& a, int32_t ydt, bool vec, int vpl, cudaStream_t st);
 // second pass of a two-pass product (FP32 Y)

@@ -157,9 +157,10 @@ bool tma_shape(int64_t nvec, int v, int team, int vpl) {
   return nvec >= 8 && (nvec & (nvec - 1)) == 0 && nvec == (int64_t)team * vpl && nvec * v <= 256 && vpl <= 2;
 }
 
-int launch_fwd(cbm_plan* P, const FwdArgs& a, int32_t xdt, int32_t ydt, bool vec, int vpl, cudaStream_t st) {
+int launch_fwd(cbm_plan* P, const FwdArgs& a, int32_t xdt, int32_t ydt, bool vec, int vpl, bool shallow,
+               cudaStream_t st) {
   if (xdt == CBM_F32) return launch_fwd_f32(P, a, vec, vpl, st);
-  return launch_fwd_bf16(P, a, ydt, vec, vpl, st);
+  return launch_fwd_bf16(P, a, ydt, vec, vpl, shallow, st);
 }
 
 template <typename T>
@@ -512,7 +513,7 @@ int matmul_impl(cbm_plan* P, int32_t op, float gin_scale, const void* x, int32_t
       // better (40 BF16 columns on the GCN graph: 0.26 -> 0.17 ms)
       if (P->variant == CBM_VARIANT_AUTO && deep_tree && !two_pass)
         a.rows_per_claim = std::min<int32_t>(a.rows_per_claim, 2);
-      rc = launch_fwd(P, a, xdt, ydt, sh.vec, vpl, st);
+      rc = launch_fwd(P, a, xdt, ydt, sh.vec, vpl, !deep_tree || two_pass, st);
     }
     if (rc) return rc;
     if (two_pass) {
