@@ -383,8 +383,13 @@ int matmul_impl(cbm_plan* P, int32_t op, float gin_scale, const void* x, int32_t
   if (!x || !y) return CBM_ERR_INVALID;
   if (ldx < n_cols || ldy < n_cols) return CBM_ERR_SHAPE;
   if (overlaps(x, extent(P->n_cols, ldx, n_cols, xdt), y, extent(P->n_rows, ldy, n_cols, ydt))) return CBM_ERR_SHAPE;
-  const bool needs_mult = op == CBM_OP_ADX || op == CBM_OP_DADX || op == CBM_OP_VALUES_RATIO || op == CBM_OP_DAD_ADD;
-  if (needs_mult && (!P->d_mult || P->n_rows != P->n_cols)) return CBM_ERR_UNSUPPORTED;
+  // column multipliers (D[col]) need a square A; the ratio rule of the VALUES
+  // op reads row multipliers only, so a rectangular plan (a row shard) may
+  // take it with one multiplier per row
+  const bool needs_col_mult = op == CBM_OP_ADX || op == CBM_OP_DADX || op == CBM_OP_DAD_ADD;
+  const bool needs_mult = needs_col_mult || op == CBM_OP_VALUES_RATIO;
+  if (needs_mult && !P->d_mult) return CBM_ERR_UNSUPPORTED;
+  if (needs_col_mult && P->n_rows != P->n_cols) return CBM_ERR_UNSUPPORTED;
   if ((op == CBM_OP_VALUES_ADD || op == CBM_OP_VALUES_RATIO) && xdt != CBM_F32) return CBM_ERR_DTYPE;
   const int64_t need = cbm_plan_workspace_bytes(P, op, n_cols, xdt, ydt, 0);
   const bool comp = comp_active(P, xdt);
