@@ -65,11 +65,13 @@ class cbm4mm:  # noqa: N801 (the reference's class name)
         cbm/cbm_extensions.cpp:498-591), with the binary A of this matrix."""
         self._plan.matmul_gin(x, y, epsilon)
 
-    def matmul_host(self, x, y, slab_cols=64):
+    def matmul_host(self, x, y, slab_cols=64, overlap_calls=False):
         """y <- (this operator) x for host tensors x and y (pinned for full-speed
         copies), the copies overlapped with the product slab by slab.  Queued on
-        the current stream: synchronise it before reading y."""
-        self._plan.matmul_host(self._op, x, y, slab_cols)
+        the current stream: synchronise it before reading y.  overlap_calls:
+        back-to-back calls also overlap one call's last copy-out with the next
+        call's first copy-in (x must be complete in host memory at the call)."""
+        self._plan.matmul_host(self._op, x, y, slab_cols, overlap_calls)
 
     @property
     def self_adjoint(self):

@@ -188,12 +188,15 @@ class Plan:
                                       ws.data_ptr(), ws.numel(), _stream(self.device))
         _lib.check(rc, "cbm_matmul_gin")
 
-    def matmul_host(self, op, x, y, slab_cols=64):
+    def matmul_host(self, op, x, y, slab_cols=64, overlap_calls=False):
         """y <- op(A) x with x and y in host memory (pinned for full-speed copies):
         column slabs are copied in, multiplied and copied out on overlapping
         streams.  Device buffers of the operand shapes are allocated on the first
         call and reused.  Returns once queued; the current stream waits for the
-        last copy (synchronise it before reading y)."""
+        last copy (synchronise it before reading y).  overlap_calls: this call's
+        copy-in may run under the previous call's last copy-out (x must then be
+        complete in host memory when the call is made; see
+        cbm_plan_set_host_overlap)."""
         op = OPS[op] if isinstance(op, str) else int(op)
         for t, rows, name in ((x, self.n_cols, "rhs"), (y, self.n_rows, "res")):
             if not isinstance(t, torch.Tensor) or t.is_cuda:
@@ -215,6 +218,8 @@ class Plan:
             self._host_bufs = bufs
         xd, yd = bufs[key]
         ws = self.workspace(op, cols, xdt, ydt, False)  # covers every slab width
+        _lib.check(self._lib.cbm_plan_set_host_overlap(self._h, 1 if overlap_calls else 0),
+                   "cbm_plan_set_host_overlap")
         rc = self._lib.cbm_matmul_host(self._h, op, x.data_ptr(), xdt, max(int(x.stride(0)), cols, 1), y.data_ptr(),
                                        ydt, max(int(y.stride(0)), cols, 1), cols, int(slab_cols), xd.data_ptr(),
                                        yd.data_ptr(), ws.data_ptr(), ws.numel(), _stream(self.device))

@@ -285,6 +285,9 @@ int build_adjoint(cbm_plan* P, cudaStream_t st) {
 void release_pipeline(cbm_plan* P) {
   for (cudaEvent_t e : P->events) cudaEventDestroy(e);
   P->events.clear();
+  if (P->host_prev_prod) cudaEventDestroy(P->host_prev_prod);
+  P->host_prev_prod = nullptr;
+  P->host_prev_valid = false;
   if (P->h2d) cudaStreamDestroy(P->h2d);
   if (P->d2h) cudaStreamDestroy(P->d2h);
   P->h2d = P->d2h = nullptr;
@@ -294,6 +297,8 @@ void release_pipeline(cbm_plan* P) {
 int pipeline_ready(cbm_plan* P, size_t n) {
   if (!P->h2d && cudaStreamCreateWithFlags(&P->h2d, cudaStreamNonBlocking) != cudaSuccess) return CBM_ERR_CUDA;
   if (!P->d2h && cudaStreamCreateWithFlags(&P->d2h, cudaStreamNonBlocking) != cudaSuccess) return CBM_ERR_CUDA;
+  if (!P->host_prev_prod && cudaEventCreateWithFlags(&P->host_prev_prod, cudaEventDisableTiming) != cudaSuccess)
+    return CBM_ERR_CUDA;
   while (P->events.size() < n) {
     cudaEvent_t e;
     if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return CBM_ERR_CUDA;
@@ -325,6 +330,12 @@ int64_t cbm_plan_workspace_bytes(const cbm_plan* P, int32_t op, int64_t n_cols, 
            (comp_active(P, x_dtype) ? P->n_internal : 0);
   }
   return align256(rows * ldp * 4) + 256;
+}
+
+int cbm_plan_set_host_overlap(cbm_plan* P, int32_t on) {
+  if (!P || (on != 0 && on != 1)) return CBM_ERR_INVALID;
+  P->host_overlap = on != 0;
+  return CBM_OK;
 }
 
 int cbm_plan_set_passes(cbm_plan* P, int32_t passes) {
@@ -581,9 +592,13 @@ int cbm_matmul_host(cbm_plan* P, int32_t op, const void* x_host, int32_t xdt, in
   if (rc) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   cudaEvent_t* ev = P->events.data();
-  // the copy streams start after the work already queued on the caller's stream
+  // the copy streams start after the work already queued on the caller's
+  // stream; with overlap across calls, the copy-in waits only until the
+  // previous call's products no longer read the device copy of X (so it runs
+  // under that call's last copy-out)
   if (cudaEventRecord(ev[0], st) != cudaSuccess) return CBM_ERR_CUDA;
-  if (cudaStreamWaitEvent(P->h2d, ev[0], 0) != cudaSuccess) return CBM_ERR_CUDA;
+  const bool overlap = P->host_overlap && P->host_prev_valid;
+  if (cudaStreamWaitEvent(P->h2d, overlap ? P->host_prev_prod : ev[0], 0) != cudaSuccess) return CBM_ERR_CUDA;
   if (cudaStreamWaitEvent(P->d2h, ev[0], 0) != cudaSuccess) return CBM_ERR_CUDA;
   const char* xh = static_cast<const char*>(x_host);
   char* yh = static_cast<char*>(y_host);
@@ -600,6 +615,10 @@ int cbm_matmul_host(cbm_plan* P, int32_t op, const void* x_host, int32_t xdt, in
     rc = cbm_matmul(P, op, xd + c0 * xs, xdt, n_cols, yd + c0 * ys, ydt, n_cols, cw, ws, ws_bytes, stream);
     if (rc) return rc;
     if (cudaEventRecord(out, st) != cudaSuccess) return CBM_ERR_CUDA;
+    if (k + 1 == n_slabs) {
+      if (cudaEventRecord(P->host_prev_prod, st) != cudaSuccess) return CBM_ERR_CUDA;
+      P->host_prev_valid = true;
+    }
     if (cudaStreamWaitEvent(P->d2h, out, 0) != cudaSuccess) return CBM_ERR_CUDA;
     if (cudaMemcpy2DAsync(yh + c0 * ys, ldy_host * ys, yd + c0 * ys, n_cols * ys, cw * ys, P->n_rows,
                           cudaMemcpyDeviceToHost, P->d2h) != cudaSuccess)

@@ -103,6 +103,12 @@ struct cbm_plan {
   // that order slabs across them, created on first use
   cudaStream_t h2d = nullptr, d2h = nullptr;
   std::vector<cudaEvent_t> events;
+  // overlap across calls (cbm_plan_set_host_overlap): the copy-in of a call
+  // waits only for the previous call's last product (recorded in
+  // host_prev_prod), not for its copy-out
+  bool host_overlap = false;
+  bool host_prev_valid = false;
+  cudaEvent_t host_prev_prod = nullptr;
 };
 
 namespace cbm {

@@ -226,6 +226,16 @@ int cbm_matmul_host(cbm_plan* plan, int32_t op, const void* x_host, int32_t x_dt
                     void* y_host, int32_t y_dtype, int64_t ldy_host, int64_t n_cols, int64_t slab_cols,
                     void* x_dev, void* y_dev, void* workspace, int64_t workspace_bytes, void* stream);
 
+/* cbm_matmul_host across calls (0: off, the default): with it on, a call's
+ * copy-in of X waits only until the previous call's products have finished
+ * reading the device copy of X, not for the previous call's copy-out, so
+ * back-to-back calls overlap one's last copy-out with the next one's first
+ * copy-in.  The copy-in is then not ordered after other work the caller
+ * queued on `stream`: x_host must be complete when the call is made (written
+ * by the host).  Results and the end-of-call guarantee (a synchronisation of
+ * `stream` makes y_host final) are unchanged. */
+int cbm_plan_set_host_overlap(cbm_plan* plan, int32_t on);
+
 /* dX = op(A)^T G (the adjoint of cbm_matmul for CBM_OP_AX/ADX/DADX): a
  * reverse tree propagation (children into parents) then a transposed delta
  * gather.  Same conventions as cbm_matmul.  No counterpart in the reference. */

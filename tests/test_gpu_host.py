@@ -54,3 +54,27 @@ def test_host_product_twice_and_errors(op_dad):
         op_dad.matmul_host(xh.cuda(), yh)
     with pytest.raises(RuntimeError):
         op_dad.matmul_host(xh, torch.empty(n, 32))
+
+
+@pytest.mark.parametrize("slab", [64, 0, 48])
+def test_back_to_back_calls_with_overlap(op_dad, slab):
+    """overlap_calls: a call's copy-in runs under the previous call's copy-out.
+    Three calls in a row on different inputs and outputs, queued without a
+    synchronisation between them, each equal to the device product; then a
+    call without overlap after them."""
+    n = op_dad.num_nodes
+    g = torch.Generator().manual_seed(slab)
+    xs = [torch.randn(n, 192, generator=g).pin_memory() for _ in range(3)]
+    ys = [torch.full((n, 192), float("nan")).pin_memory() for _ in range(3)]
+    for x, y in zip(xs, ys):
+        op_dad.matmul_host(x, y, slab_cols=slab, overlap_calls=True)
+    last = torch.full((n, 192), float("nan")).pin_memory()
+    op_dad.matmul_host(xs[0], last, slab_cols=slab)
+    torch.cuda.current_stream().synchronize()
+    ref = torch.empty(n, 192, device="cuda")
+    for x, y in zip(xs, ys):
+        op_dad.matmul(x.cuda(), ref)
+        assert torch.equal(y, ref.cpu())
+    op_dad.matmul(xs[0].cuda(), ref)
+    assert torch.equal(last, ref.cpu())
+    op_dad.plan.check_device()
