@@ -1537,6 +1537,78 @@ __device__ __forceinline__ void gather_dual(float (&acc)[VPL][V], const GT* __re
   }
 }
 
+// acc += sum over entries of s * (internal ? H[slot] : scale * G[row]) with the
+// whole warp on one entry range: G = 32 / TL groups of TL lanes, group g takes
+// the entries g, g + G, g + 2G, ... of each batch of 32, and the groups' sums
+// are added at the end (shuffles across the group bits), so every lane holds
+// the total.  Rows narrower than a warp then keep all 32 lanes on one column
+// instead of splitting the warp between columns whose lists differ in length.
+// The sum's order differs from the one-team order; the adjoint is held to
+// FP64 and finite-difference bounds, not to the forward's order.
+template <typename GT, int VPL, int V>
+__device__ __forceinline__ void gather_dual_split(float (&acc)[VPL][V], const GT* __restrict__ g, int64_t ldg,
+                                                  const float* __restrict__ h, int ldp, int nvec,
+                                                  const uint32_t* __restrict__ ent, int64_t beg, int64_t end,
+                                                  const float* __restrict__ mult, bool scale_g, int lane, int TL) {
+  constexpr int U = unroll_for<VPL, V>();
+  const int grp = lane / TL;
+  const int tl = lane & (TL - 1);
+  const int G = 32 / TL;
+  for (int64_t base = beg; base < end; base += 32) {
+    const int64_t idx = base + lane;
+    uint32_t e = 0;
+    float sc = 0.f;
+    if (idx < end) {
+      e = __ldg(ent + idx);
+      const uint32_t r = e & kIndexMask;
+      const float sgn = (e >> 31) ? -1.f : 1.f;
+      sc = (e & kInternalBit) ? sgn : (scale_g ? sgn * __ldg(mult + r) : sgn);
+    }
+    const int cnt = (int)((end - base) < 32 ? (end - base) : 32);
+    for (int j = 0; j < cnt; j += G * U) {  // the same trip count on every lane
+      float buf[U][VPL][V];
+      float s[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int jj = j + u * G + grp;
+        const uint32_t eu = __shfl_sync(0xffffffffu, e, jj < cnt ? jj : 0);
+        s[u] = __shfl_sync(0xffffffffu, sc, jj < cnt ? jj : 0);
+        const uint32_t r = eu & kIndexMask;
+        const bool in = (eu & kInternalBit) != 0;
+#pragma unroll
+        for (int v = 0; v < VPL; ++v) {
+          const int vi = tl + v * TL;
+          if (jj < cnt && vi < nvec) {
+            if (in) {
+              load_f32_cg<V>(h + (int64_t)r * ldp + vi * V, buf[u][v]);
+            } else {
+              Vec<GT, V>::load(g + (int64_t)r * ldg + (int64_t)vi * V, buf[u][v]);
+            }
+          } else {
+#pragma unroll
+            for (int k = 0; k < V; ++k) buf[u][v][k] = 0.f;
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (j + u * G + grp < cnt) {
+#pragma unroll
+          for (int v = 0; v < VPL; ++v)
+#pragma unroll
+            for (int k = 0; k < V; ++k) acc[v][k] = fmaf(s[u], buf[u][v][k], acc[v][k]);
+        }
+      }
+    }
+  }
+  for (int off = TL; off < 32; off <<= 1) {
+#pragma unroll
+    for (int v = 0; v < VPL; ++v)
+#pragma unroll
+      for (int k = 0; k < V; ++k) acc[v][k] += __shfl_xor_sync(0xffffffffu, acc[v][k], off);
+  }
+}
+
 template <typename GT, int VPL, int V>
 __global__ void __launch_bounds__(kThreads) rev_kernel(const RevArgs a) {
   const int lane = threadIdx.x & 31;
@@ -1614,14 +1686,17 @@ __global__ void __launch_bounds__(kThreads) rev_kernel(const RevArgs a) {
   finish_block(a.qs, epoch);
 }
 
-template <typename GT, typename DT, int VPL, int V>
+// SPLIT (rows narrower than a warp): one item per warp, its entries spread
+// over the warp's lane groups (gather_dual_split); group 0 writes the result.
+template <typename GT, typename DT, int VPL, int V, bool SPLIT = false>
 __global__ void __launch_bounds__(kThreads) tr_kernel(const TrArgs a) {
   const int lane = threadIdx.x & 31;
   const int TL = a.team;
-  const int team = lane / TL;
+  const int team = SPLIT ? 0 : lane / TL;
   const int tl = lane & (TL - 1);
-  const int teams = 32 / TL;
-  const unsigned tmask = (TL == 32) ? 0xffffffffu : (((1u << TL) - 1u) << (team * TL));
+  const int teams = SPLIT ? 1 : 32 / TL;
+  const bool writer = !SPLIT || lane < TL;
+  const unsigned tmask = (SPLIT || TL == 32) ? 0xffffffffu : (((1u << TL) - 1u) << (team * TL));
   const unsigned epoch = *(volatile unsigned*)&a.qs->epoch + 1u;
   const GT* g = static_cast<const GT*>(a.g);
   if (a.n_chunks > 0) {
@@ -1637,18 +1712,23 @@ __global__ void __launch_bounds__(kThreads) tr_kernel(const TrArgs a) {
         for (int v = 0; v < VPL; ++v)
 #pragma unroll
           for (int q = 0; q < V; ++q) acc[v][q] = 0.f;
-        gather_dual<GT, VPL, V>(acc, g, a.ldg, a.h, a.ldp, a.nvec, a.ent, a.chunk_beg[k], a.chunk_end[k],
-                                a.mult, a.scale_g != 0, true, nullptr, epoch, a.qs, a.timeout_ns, tl, TL,
-                                tmask);
+        if constexpr (SPLIT) {
+          gather_dual_split<GT, VPL, V>(acc, g, a.ldg, a.h, a.ldp, a.nvec, a.ent, a.chunk_beg[k], a.chunk_end[k],
+                                        a.mult, a.scale_g != 0, lane, TL);
+        } else {
+          gather_dual<GT, VPL, V>(acc, g, a.ldg, a.h, a.ldp, a.nvec, a.ent, a.chunk_beg[k], a.chunk_end[k],
+                                  a.mult, a.scale_g != 0, true, nullptr, epoch, a.qs, a.timeout_ns, tl, TL,
+                                  tmask);
+        }
         float* prow = a.partial + (int64_t)k * a.ldp;
 #pragma unroll
         for (int v = 0; v < VPL; ++v) {
           const int vi = tl + v * TL;
-          if (vi < a.nvec) store_f32<V>(prow + vi * V, acc[v]);
+          if (writer && vi < a.nvec) store_f32<V>(prow + vi * V, acc[v]);
         }
         __threadfence();
         __syncwarp(tmask);
-        if (tl == 0) st_release(a.chunk_flag + k, epoch);
+        if (SPLIT ? lane == 0 : tl == 0) st_release(a.chunk_flag + k, epoch);
       }
       __syncwarp();
     }
@@ -1669,8 +1749,13 @@ __global__ void __launch_bounds__(kThreads) tr_kernel(const TrArgs a) {
         for (int q = 0; q < V; ++q) acc[v][q] = 0.f;
       const int c0 = a.chunk0[item];
       if (c0 < 0) {
-        gather_dual<GT, VPL, V>(acc, g, a.ldg, a.h, a.ldp, a.nvec, a.ent, a.ptr[item], a.ptr[item + 1], a.mult,
-                                a.scale_g != 0, true, nullptr, epoch, a.qs, a.timeout_ns, tl, TL, tmask);
+        if constexpr (SPLIT) {
+          gather_dual_split<GT, VPL, V>(acc, g, a.ldg, a.h, a.ldp, a.nvec, a.ent, a.ptr[item], a.ptr[item + 1],
+                                        a.mult, a.scale_g != 0, lane, TL);
+        } else {
+          gather_dual<GT, VPL, V>(acc, g, a.ldg, a.h, a.ldp, a.nvec, a.ent, a.ptr[item], a.ptr[item + 1], a.mult,
+                                  a.scale_g != 0, true, nullptr, epoch, a.qs, a.timeout_ns, tl, TL, tmask);
+        }
       } else {
         for (int k = c0; k < a.n_chunks && a.chunk_item[k] == (int)item; ++k) {
           if (!wait_flag(a.chunk_flag + k, epoch, a.qs, a.timeout_ns, (long long)k)) continue;
@@ -1694,7 +1779,7 @@ __global__ void __launch_bounds__(kThreads) tr_kernel(const TrArgs a) {
 #pragma unroll
       for (int v = 0; v < VPL; ++v) {
         const int vi = tl + v * TL;
-        if (vi < a.nvec) {
+        if (writer && vi < a.nvec) {
           if (a.scale_out) {
 #pragma unroll
             for (int q = 0; q < V; ++q) acc[v][q] = __fmul_rn(acc[v][q], so);

@@ -141,10 +141,10 @@ int launch_rev_t(cbm_plan* P, const RevArgs& a, cudaStream_t st) {
   return cuda_status(cudaGetLastError());
 }
 
-template <typename GT, typename DT, int VPL, int V>
+template <typename GT, typename DT, int VPL, int V, bool SPLIT = false>
 int launch_tr_t(cbm_plan* P, const TrArgs& a, cudaStream_t st) {
   static GridCache cache;
-  auto kern = tr_kernel<GT, DT, VPL, V>;
+  auto kern = tr_kernel<GT, DT, VPL, V, SPLIT>;
   const int grid = cached_grid(cache, kern, P->device, kThreads, 0);
   if (grid <= 0) return CBM_ERR_CUDA;
   kern<<<grid, kThreads, 0, st>>>(a);

@@ -2,8 +2,13 @@
 #include "launch.cuh"
 
 namespace cbm {
+// Rows narrower than a warp (teams of 1-16 lanes, one vector per lane) take
+// the split kernel: the warp's lane groups share one column's entries.
+constexpr bool kTrSplitNarrow = true;
+
 template <typename GT, typename DT, int V>
 int launch_tr_v(cbm_plan* P, const TrArgs& a, int vpl, cudaStream_t st) {
+  if (kTrSplitNarrow && vpl == 1 && a.team < 32) return launch_tr_t<GT, DT, 1, V, true>(P, a, st);
   switch (vpl) {
     case 1: return launch_tr_t<GT, DT, 1, V>(P, a, st);
     case 2: return launch_tr_t<GT, DT, 2, V>(P, a, st);
