@@ -736,6 +736,27 @@ def main():
     e1.record(stream)
     barrier()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1) / e2e_steps, dev)
+    # the PCIe bound of one step: the same bytes copied in and out at once
+    # (pinned host <-> HBM, one stream each way) with no product; x and y
+    # get back the values they hold
+    s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+    copy_ms = []
+    for i in range(5):
+        c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c0.record(stream)
+        s_in.wait_stream(stream)
+        s_out.wait_stream(stream)
+        with torch.cuda.stream(s_in):
+            x.copy_(xh, non_blocking=True)
+        with torch.cuda.stream(s_out):
+            yh.copy_(y, non_blocking=True)
+        stream.wait_stream(s_in)
+        stream.wait_stream(s_out)
+        c1.record(stream)
+        c1.synchronize()
+        if i >= 2:
+            copy_ms.append(c0.elapsed_time(c1))
+    copy_ms = max_over_ranks(statistics.mean(copy_ms), dev)
 
     if rank == 0:
         kernel_ms = statistics.mean(per)
@@ -763,6 +784,8 @@ def main():
             "e2e": {"value": b_alg * world / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s",
                     "h2d_bytes_per_step": int(xh.numel() * 4), "d2h_bytes_per_step": int(yh.numel() * 4),
                     "ms_per_step": e2e_ms,
+                    "copy_bound_ms": copy_ms,
+                    "frac_of_copy_bound": copy_ms / e2e_ms,
                     "api": "cbm4dad.matmul_host (pinned host X and Y, overlap_calls=True)",
                     "slab_cols": args.slab_cols},
             "gpu_launches": int(launches),
