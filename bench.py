@@ -17,10 +17,9 @@ plain FP32, and their ratio (rank 0 only).
 At N = 1 the line also carries the other forms, each measured on the device
 with CUDA events after its own warm-up, outside the headline's timed region:
 "precision" (A D^-1/2 X on the 2.4M-node workload, X stored BF16), "batch"
-(the 512-graph workload in one launch replayed from a CUDA graph) and
-"reference_gpu" (the reference's own cusparseCBM.matmul_DAX_DADX, compiled
-from its source, on the headline's structure), with error against FP64 on
-sampled rows.
+(the 512-graph workload in one launch replayed from a CUDA graph) and "small"
+(A.X on the 4,096-node community graph: launch latency, eager and from a CUDA
+graph), with error against FP64 on sampled rows.
 
 N > 1 runs under torchrun, one rank per GPU: each rank owns a 256-column shard
 of X and Y (column sharding needs no collective; weak scaling).  Rank 0
@@ -28,7 +27,9 @@ prints one JSON line.  ``--impl reference`` times the reference's CPU product
 path (MKL CSR SpMM + OpenMP branch-serial fused update,
 s_spmm_fused_update_csr_int32, cbm/cbm_extensions.cpp:593-698), compiled from
 its source into oracle/_ref/ (else the oracle's restatement of it), on all
-host threads.
+host threads; its line also carries "reference_gpu", the reference's own GPU
+products (cusparseCBM, compiled from cbm/cbm.cu) on the headline workload and
+on the 4,096-node graph, timed with CUDA events on the same box.
 """
 from __future__ import annotations
 
@@ -318,6 +319,10 @@ def run_reference(args, rank, world):
             "cpu_baseline": {"value": v, "unit": "GB/s", "cores": host_threads(), "kind": kind,
                              "sample": f"every step one full product of the workload: {what}"},
             "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if not args.no_forms:
+        # context beside the CPU arm: the reference's GPU path on this box
+        line["reference_gpu"] = _form(lambda: reference_gpu_timing(
+            args.steps, args.warmup, (n, crow, col, val, s.branches, s.src, s.dst, dinv, x, b_alg)))
     print(json.dumps(line), flush=True)
 
 
@@ -523,31 +528,96 @@ def run_precision(args):
     print(json.dumps(line), flush=True)
 
 
-def reference_gpu_form(a, x, y_ours, steps, warmup):
-    """The reference's own GPU product cusparseCBM.matmul_DAX_DADX (cbm/cbm.cu:210-268:
-    cuSPARSE SpMM, then its fused_update kernel), compiled from its source into
-    oracle/_ref/, on the headline's structure and X: ms per product, its
-    algorithmic-byte rate, and its agreement with this library's result
-    (rtol 1e-5, atol 1e-6)."""
+def small_form(steps, warmup):
+    """The 4,096-node community graph (64 communities of 64, 12 in-community
+    and 4 uniform neighbours, seed 0, alpha 0): A.X with X FP32 U[-1, 1],
+    4096 x 64.  The operands (1 MB) sit in L2, so this times launch latency,
+    not memory: one eager call and one CUDA-graph replay of the same call.
+    The reference's GPU path on the same graph is timed by --impl reference."""
+    from cbm import synthetic
+    from cbm.cbm4mm import cbm4mm
+
+    ei, n, spec = synthetic.workload("community-4096")
+    a = cbm4mm(torch.from_numpy(ei), torch.ones(ei.shape[1]), alpha=0)
+    g = torch.Generator(device="cuda").manual_seed(0)
+    x = torch.rand(n, 64, device="cuda", generator=g) * 2 - 1
+    y = torch.empty_like(x)
+    st = a.plan.stats
+    b_alg = bytes_alg(n, st["nnz"], st["edges"], st["branches"], 64, scaled=False)
+    reps = 20  # products per timed replay or loop, so each event pair spans many launches
+    eager_ms = _time_events(lambda: [a.matmul(x, y) for _ in range(reps)], steps, warmup) / reps
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        for _ in range(3):
+            a.matmul(x, y)
+    torch.cuda.current_stream().wait_stream(s)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        for _ in range(reps):
+            a.matmul(x, y)
+    graph_ms = _time_events(graph.replay, steps, warmup) / reps
+    out = {"workload": "community-4096 A.X (c0 shape: 4096 nodes, 64 FP32 columns, alpha 0)", "nodes": n,
+           "nnz_a": int(a.structure_stats["nnz_a"]), "nnz_delta": int(st["nnz"]),
+           "eager_us": eager_ms * 1e3, "graph_replay_us": graph_ms * 1e3,
+           "graph_replay_gbs": b_alg / (graph_ms * 1e-3) / 1e9,
+           "note": "L2-resident and launch-bound: no roofline claim"}
+    a.plan.check_device()
+    return out
+
+
+def reference_gpu_timing(steps, warmup, headline):
+    """The reference's own GPU products (cbm/cbm.cu, compiled from its source
+    into oracle/_ref/ by oracle/build_ref.py), timed with CUDA events on the
+    structures this arm's CPU leg uses: matmul_DAX_DADX (cuSPARSE SpMM, then
+    its fused_update kernel) on the headline workload, and matmul_AX_ADX on the
+    4,096-node community graph (A.X, 64 FP32 columns, eager: its per-call
+    allocations keep it out of CUDA graphs).  ``headline`` = (n, crow, col,
+    val, branches, src, dst, dinv, x, b_alg) as host arrays."""
     from oracle import build_ref
 
+    if not torch.cuda.is_available():
+        return {"unavailable": "no GPU"}
     mod = build_ref.load("cbm_cusparse_ref")
     if mod is None:
         return {"unavailable": "the reference's GPU module was not built (no reference tree at build time)"}
-    n = a.num_nodes
-    br = a.mca_offset
-    # the reference's update kernel reads one branch offset past the end
-    # (one block per entry of mca_branches, cbm/cbm.cu:136, :193): hand it a
-    # view of a buffer with a readable sentinel equal to the edge count
-    br_pad = torch.cat([br, br[-1:]])[: br.numel()]
-    csr = torch.sparse_csr_tensor(a.deltas.crow_indices(), a.deltas.col_indices(), a.deltas.values(), (n, n))
-    ref = mod.cusparseCBM(csr, br_pad, a.mca_src_idx, a.mca_dst_idx, a.D)
-    y = torch.empty_like(x)
-    ms = _time_events(lambda: ref.matmul_DAX_DADX(x, y), steps, warmup)
-    agree = bool(torch.allclose(y, y_ours, rtol=1e-5, atol=1e-6))
-    del ref
-    return {"impl": "reference cusparseCBM.matmul_DAX_DADX (cbm/cbm.cu), built from its source for sm_100a",
-            "ms": ms, "steps": steps, "warmup": warmup, "agrees_rtol1e-5_atol1e-6": agree}
+    dev = torch.device("cuda")
+
+    def make(n, crow, col, val, br, src, dst, mult):
+        t = lambda a, d: torch.from_numpy(np.ascontiguousarray(a, dtype=d)).to(dev)
+        csr = torch.sparse_csr_tensor(t(crow, np.int32), t(col, np.int32), t(val, np.float32), (n, n))
+        # its update kernel reads one branch offset past the end (one block per
+        # entry of mca_branches, cbm/cbm.cu:136, :193): a view of a buffer with
+        # a readable sentinel equal to the edge count
+        brp = t(np.append(br, br[-1]), np.int32)[: len(br)]
+        m = t(mult, np.float32) if mult is not None else torch.empty(0, device=dev)
+        s_t, d_t = t(src, np.int32), t(dst, np.int32)
+        # the extension keeps raw pointers to every tensor it is given
+        # (cbm/cbm.cu:110-140): all of them must outlive it
+        return mod.cusparseCBM(csr, brp, s_t, d_t, m), (csr, brp, m, s_t, d_t)
+
+    out = {"impl": "reference cusparseCBM (cbm/cbm.cu), built from its source for sm_100a"}
+    n, crow, col, val, br, src, dst, dinv, x, b_alg = headline
+    ref, keep = make(n, crow, col, val, br, src, dst, dinv)
+    xt = torch.from_numpy(x).to(dev)
+    y = torch.empty_like(xt)
+    ms = _time_events(lambda: ref.matmul_DAX_DADX(xt, y), max(steps, 10), max(warmup, 3))
+    out["headline"] = {"call": "matmul_DAX_DADX", "ms": ms, "value": b_alg / (ms * 1e-3) / 1e9, "unit": "GB/s"}
+    del ref, keep, xt, y
+    from cbm import cbm_mkl_cpp, synthetic
+
+    ei, n, _ = synthetic.workload("community-4096")
+    st = cbm_mkl_cpp.build(ei[0], ei[1], n, 0)
+    ref, keep = make(n, st.csr_ptr, st.csr_col, st.csr_val, st.branches, st.src, st.dst, None)
+    g = torch.Generator(device="cuda").manual_seed(0)
+    xs = torch.rand(n, 64, device=dev, generator=g) * 2 - 1
+    ys = torch.empty_like(xs)
+    reps = 20
+    ms = _time_events(lambda: [ref.matmul_AX_ADX(xs, ys) for _ in range(reps)], max(steps, 10),
+                      max(warmup, 3)) / reps
+    out["small"] = {"call": "matmul_AX_ADX", "workload": "community-4096 A.X, 64 FP32 columns", "us": ms * 1e3}
+    del ref, keep
+    return out
 
 
 def run_lsh(args):
@@ -623,7 +693,7 @@ def main():
     ap.add_argument("--no-forms", action="store_true",
                     help="leave the precision, batch and reference-GPU records out of the headline line")
     ap.add_argument("--gcn-only", action="store_true", help="only the GCN timing (one JSON object)")
-    ap.add_argument("--workload", default="headline", choices=["headline", "batch", "precision", "lsh"],
+    ap.add_argument("--workload", default="headline", choices=["headline", "batch", "precision", "lsh", "small"],
                     help="batch / precision / lsh: the batching, precision or LSH-clustered form instead of "
                          "the headline line")
     ap.add_argument("--max-cluster", type=int, default=100000, help="lsh workload: cluster size bound")
@@ -658,7 +728,9 @@ def main():
 
     if args.workload != "headline":
         if rank == 0:
-            {"batch": run_batch, "precision": run_precision, "lsh": run_lsh}[args.workload](args)
+            {"batch": run_batch, "precision": run_precision, "lsh": run_lsh,
+             "small": lambda a: print(json.dumps(small_form(a.steps, max(a.warmup, 3))), flush=True)}[
+                args.workload](args)
         return
     if args.gcn_only:
         if rank == 0:
@@ -793,14 +865,6 @@ def main():
             "plan": a.plan.stats,
             "error_vs_fp64": err,
         }
-        if world == 1 and not args.no_forms:
-            line["reference_gpu"] = _form(lambda: reference_gpu_form(a, x, y, max(args.steps, 10), args.warmup))
-            if "ms" in line["reference_gpu"]:
-                r = line["reference_gpu"]
-                r["value"] = b_alg / (r["ms"] * 1e-3) / 1e9
-                r["unit"] = "GB/s"
-                r["ours_ms"] = kernel_ms
-                r["speedup_ours_over_reference"] = r["ms"] / kernel_ms
         if not args.no_gcn:
             line["gcn"] = gcn_timing(max(args.steps, 10), max(args.warmup, 3))
         if world == 1 and not args.no_cpu_baseline:
@@ -813,6 +877,7 @@ def main():
                                                                     "rows_per_claim": [8, 16]}))
             torch.cuda.empty_cache()
             line["batch"] = _form(lambda: batch_form(max(args.steps, 10), args.warmup))
+            line["small"] = _form(lambda: small_form(max(args.steps, 10), max(args.warmup, 3)))
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.barrier()
