@@ -39,6 +39,7 @@ import os
 import statistics
 import subprocess
 import sys
+import threading
 import time
 
 import numpy as np
@@ -149,17 +150,58 @@ def dinv_f64(ei, n):
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """SM clock, power and clock-event reasons sampled DURING the timed region:
+    through NVML every 2 ms from a thread (nvidia_ml_py), else nvidia-smi
+    every 200 ms.  Read-only: no clock or other setting is changed."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits and their nvidia-smi names
+    REASONS = ((0x8, "hw_slowdown"), (0x40, "hw_thermal_slowdown"), (0x20, "sw_thermal_slowdown"),
+               (0x4, "sw_power_cap"), (0x80, "hw_power_brake_slowdown"))
 
     def __init__(self, index):
         self.index = index
         self.proc = None
+        self.thread = None
+        self.rows = []
+        self.out = ""
+
+    def _nvml(self):
+        import pynvml
+
+        pynvml.nvmlInit()
+        try:
+            u = str(torch.cuda.get_device_properties(self.index).uuid)
+            h = pynvml.nvmlDeviceGetHandleByUUID((u if u.startswith("GPU-") else "GPU-" + u).encode())
+        except Exception:
+            ids = [v.strip() for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip()]
+            idx = int(ids[self.index]) if len(ids) > self.index and ids[self.index].isdigit() else self.index
+            h = pynvml.nvmlDeviceGetHandleByIndex(idx)
+        return pynvml, h
 
     def __enter__(self):
+        try:
+            nv, h = self._nvml()
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.stop = threading.Event()
+
+            def loop():
+                while not self.stop.is_set():
+                    try:
+                        self.rows.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                                          nv.nvmlDeviceGetPowerUsage(h) / 1000.0,
+                                          int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))))
+                    except Exception:
+                        return
+                    self.stop.wait(0.002)
+
+            self.thread = threading.Thread(target=loop, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.thread = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
@@ -170,7 +212,10 @@ class Clocks:
         return self
 
     def __exit__(self, *a):
-        self.out = ""
+        if self.thread is not None:
+            self.stop.set()
+            self.thread.join(timeout=5)
+            return
         if self.proc is not None:
             time.sleep(0.25)
             self.proc.terminate()
@@ -180,6 +225,16 @@ class Clocks:
                 self.proc.kill()
 
     def summary(self):
+        if self.thread is not None:
+            if not self.rows:
+                return None
+            bits = 0
+            for r in self.rows:
+                bits |= r[2]
+            return {"sm_mhz": statistics.median(r[0] for r in self.rows), "sm_max_mhz": self.max_mhz,
+                    "sm_min_mhz": min(r[0] for r in self.rows), "power_w_median": statistics.median(r[1] for r in self.rows),
+                    "samples": len(self.rows), "source": "NVML every 2 ms inside the timed region",
+                    "reasons": sorted(name for bit, name in self.REASONS if bits & bit)}
         rows = []
         for line in (self.out or "").splitlines():
             parts = [p.strip() for p in line.split(",")]
@@ -195,7 +250,7 @@ class Clocks:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in loaded for i, v in enumerate(r[3]) if v.lower() == "active"})
         return {"sm_mhz": statistics.median(r[0] for r in loaded), "sm_max_mhz": max(r[1] for r in rows),
-                "samples": len(rows), "reasons": reasons}
+                "samples": len(rows), "source": "nvidia-smi every 200 ms", "reasons": reasons}
 
 
 def traffic_from_profile():
