@@ -472,7 +472,7 @@ int matmul_impl(cbm_plan* P, int32_t op, float gin_scale, const void* x, int32_t
     a.scale_mode = scale;
     a.prop_mode = prop;
     a.team = team;
-    a.rows_per_claim = P->rows_per_claim;
+    a.rows_per_claim = claim_rows(P);
     a.rows_per_claim_deep = deep_rows_per_claim(P);
     a.n_root = (int32_t)P->n_root;
     a.unit = P->d_unit;
@@ -716,7 +716,7 @@ int cbm_matmul_adjoint(cbm_plan* P, int32_t op, const void* g, int32_t gdt, int6
     t.nvec = (int32_t)nvec;
     t.partial = partial;
     t.team = team;
-    t.rows_per_claim = P->rows_per_claim;
+    t.rows_per_claim = claim_rows(P);
     t.timeout_ns = P->timeout_ns;
     if ((rc = launch_tr(P, t, gdt, ddt, sh.vec, vpl, st))) return rc;
   }

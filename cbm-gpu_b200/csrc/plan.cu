@@ -195,12 +195,22 @@ int build_layout(cbm_plan* P, cudaStream_t st) {
   return cuda_status(cudaStreamSynchronize(st));
 }
 
+// Level-0 rows a team takes per claim: rows_per_claim, cut down on plans with
+// fewer rows than that many per resident warp of the GPU (64 per SM).  A
+// team's rows run one after another, so a small plan spreads them one per
+// team instead (4,096 rows, 64 FP32 columns: 52 -> 17 us per product).
+int32_t claim_rows(const cbm_plan* P) {
+  const int64_t warps = (int64_t)sm_count(P->device) * 64;
+  const int64_t fit = P->n_items / std::max<int64_t>(warps, 1);
+  return (int32_t)std::max<int64_t>(1, std::min<int64_t>(P->rows_per_claim, fit));
+}
+
 // Rows below level 0 wait on parents claimed just before them; when they are a
 // large share of the rows, one-row claims keep that chain short.  Otherwise
 // their parents are long finished and larger claims cost less.
 int32_t deep_rows_per_claim(const cbm_plan* P) {
   if (P->rows_per_claim_deep > 0) return P->rows_per_claim_deep;
-  return (P->n_items - P->n_root) * 4 > P->n_items ? 1 : P->rows_per_claim;
+  return (P->n_items - P->n_root) * 4 > P->n_items ? 1 : claim_rows(P);
 }
 
 // Claim units of the staged kernel.  Level-0 items (which wait on nothing) are
@@ -225,7 +235,7 @@ int build_units(cbm_plan* P, cudaStream_t st) {
   };
   double total = 0;
   for (int64_t i = 0; i < nr; ++i) total += (double)cost(i);
-  const double target = nr > 0 ? P->rows_per_claim * total / (double)nr : 0.0;
+  const double target = nr > 0 ? claim_rows(P) * total / (double)nr : 0.0;
   std::vector<int32_t> unit(1, 0);
   int64_t i = 0;
   while (i < nr) {

@@ -116,7 +116,9 @@ int cuda_status(cudaError_t e);
 void free_all(std::vector<void*>& v);
 int build_layout(cbm_plan* P, cudaStream_t st);
 int build_units(cbm_plan* P, cudaStream_t st);
+int32_t claim_rows(const cbm_plan* P);
 int32_t deep_rows_per_claim(const cbm_plan* P);
+int sm_count(int device);
 int rebuild_adjoint_chunks(cbm_plan* P, cudaStream_t st);
 void release_pipeline(cbm_plan* P);
 int transpose_on_device(cbm_plan* P, cudaStream_t st);
