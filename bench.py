@@ -383,7 +383,8 @@ def run_reference(args, rank, world):
 
 def gcn_timing(steps, warmup):
     """2-layer GCN (128 -> 256 -> 40) on the 170,000-node power-law graph: forward +
-    backward ms per step, BF16 activations vs plain FP32 (cbm4dad adjacency)."""
+    backward ms per step, BF16 activations vs plain FP32 (cbm4dad adjacency),
+    eager and replayed from a CUDA graph of the whole step."""
     from cbm import _lib, synthetic
     from cbm.cbm4dad import cbm4dad
     from cbm.gcn import GCN, cross_entropy
@@ -417,6 +418,21 @@ def gcn_timing(steps, warmup):
         torch.cuda.synchronize()
         out[f"{name}_ms"] = e0.elapsed_time(e1) / steps
         out[f"{name}_cbm_launches_per_step"] = (a.plan.stat(_lib.P_LAUNCHES) - l0) / steps
+        # the same step captured once as a CUDA graph (forward, loss and
+        # backward; the weight gradients are the graph's outputs) and replayed
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            for _ in range(3):
+                step()
+        torch.cuda.current_stream().wait_stream(s)
+        model.w1.grad = None
+        model.w2.grad = None
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            cross_entropy(model(xin), labels).backward()
+        out[f"{name}_graph_ms"] = _time_events(graph.replay, steps, warmup)
+        del graph
         # the step's CBM work alone: Ahat X (128 columns), Ahat (H W2) (40 columns,
         # FP32 out) and the adjoint of the latter, on the step's dtypes
         x_act = xin
