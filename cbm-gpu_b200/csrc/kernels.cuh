@@ -33,6 +33,11 @@ constexpr int kThreads = 256;
 constexpr uint32_t kColMask = 0x3fffffffu;
 constexpr uint32_t kHotBit = 0x40000000u;
 
+// Element offset of row r with leading dimension ld (below 2^31, which the
+// host checks): one widening 32 x 32 -> 64-bit multiply per gathered row
+// instead of a 64-bit one.
+__device__ __forceinline__ uint64_t row_off(uint32_t r, int64_t ld) { return (uint64_t)r * (uint32_t)ld; }
+
 enum ScaleMode : int {
   SCALE_SIGN = 0,       // s
   SCALE_DCOL = 1,       // s * m[col]
@@ -313,7 +318,7 @@ __device__ __forceinline__ void gather_range(float (&acc)[VPL][V], const XT* __r
       for (int u = 0; u < U; ++u) {
         const uint32_t eu = __shfl_sync(tmask, e, j + u < cnt ? j + u : 0, TL);
         s[u] = __shfl_sync(tmask, sc, j + u < cnt ? j + u : 0, TL);
-        const XT* row = x + (int64_t)(eu & kColMask) * ldx;
+        const XT* row = x + row_off(eu & kColMask, ldx);
 #pragma unroll
         for (int v = 0; v < VPL; ++v) {
           const int vi = tl + v * TL;
@@ -815,7 +820,7 @@ __device__ __forceinline__ float entry_scale(uint32_t e, int64_t idx, bool valid
 // current item ends (INT_MAX when none is left); on_end(acc) finishes it,
 // resets acc and advances, updating row_dv (the row factor: m[row] under
 // SCALE_DCOL_DROW, exactly 1 otherwise).
-template <typename XT, int TL, int VPL, int V, int S, int BLOCK, typename NextEnd, typename OnEnd>
+template <typename XT, int TL, int VPL, int V, int S, int BLOCK, bool OFF32, typename NextEnd, typename OnEnd>
 __device__ __forceinline__ void stream_pass(const XT* __restrict__ x, int64_t ldx, int nvec,
                                             const uint32_t* __restrict__ ent, const float* __restrict__ val,
                                             int64_t k0, int len, int scale_mode, const float* __restrict__ mult,
@@ -850,23 +855,36 @@ __device__ __forceinline__ void stream_pass(const XT* __restrict__ x, int64_t ld
     sA = entry_scale(eA, ia, ia < len, scale_mode, mult, val0);
     sB = entry_scale(eB, ib, ib < len, scale_mode, mult, val0);
   }
+  // X row of entry word e from a lane's base: with OFF32 (X holds fewer than
+  // 2^32 elements) a 32-bit element offset and one scaled add, else 64-bit
+  auto row_at = [&](const XT* base, uint32_t e) -> const XT* {
+    if constexpr (OFF32) {
+      return base + (uint32_t)((e & kColMask) * (uint32_t)ldx);
+    } else {
+      return base + row_off(e & kColMask, ldx);
+    }
+  };
   // entry p's pieces into ring slot sp (no commit).  One piece per lane
-  // (narrow rows): branch-free, a piece outside the row or an entry past the
-  // stream's end (its word is 0, so the address is X's first row) copies 0
-  // bytes and zero-fills the slot.  Several pieces per lane: pieces outside
-  // the row and entries past the end are skipped (the slots keep old data,
-  // never read).
+  // (narrow rows): branch-free.  An entry past the stream's end (its word is
+  // 0, so the address is X's first row) copies 0 bytes and zero-fills the
+  // slot.  A lane without a piece (a row narrower than the team) copies the
+  // first 16 bytes of the row, a valid address, into a slot whose sums no
+  // store reads (every store is limited to the row's pieces); so the
+  // per-entry code tests only the stream's end, with a constant size.
+  // Several pieces per lane: pieces outside the row and entries past the end
+  // are skipped (the slots keep old data, never read).
+  const XT* xp = piece_ok[0] ? xl : x;
   auto produce = [&](int p, uint4* sp) {
     if constexpr (VPL == 1) {
       const bool inA = p < bA + TL;
       const uint32_t e = __shfl_sync(tmask, inA ? eA : eB, p & (TL - 1), TL);
-      const XT* row = xl + (int64_t)(e & kColMask) * ldx;
+      const XT* row = row_at(xp, e);
       const uint64_t pol = (e & kHotBit) ? pol_keep : pol_stream;
-      cp_async16_hint_n(sp, piece_ok[0] ? row : x, (p < len && piece_ok[0]) ? 16u : 0u, pol);
+      cp_async16_hint_n(sp, row, p < len ? 16u : 0u, pol);
     } else if (p < len) {
       const bool inA = p < bA + TL;
       const uint32_t e = __shfl_sync(tmask, inA ? eA : eB, p & (TL - 1), TL);
-      const XT* row = xl + (int64_t)(e & kColMask) * ldx;
+      const XT* row = row_at(xl, e);
       const uint64_t pol = (e & kHotBit) ? pol_keep : pol_stream;
 #pragma unroll
       for (int v = 0; v < VPL; ++v)
@@ -929,8 +947,8 @@ __device__ __forceinline__ void stream_pass(const XT* __restrict__ x, int64_t ld
     if (k + U <= len && end_at >= k + U) {
       // row_dv is m[row] under SCALE_DCOL_DROW and exactly 1 otherwise
       if constexpr (VPL == 1) {
-        // all U scales, then all U pieces, then the FMAs (the zero-filled
-        // pieces of lanes outside the row add zeros to unused accumulators)
+        // all U scales, then all U pieces, then the FMAs (lanes outside the
+        // row add their placeholder pieces to accumulators no store reads)
         float sc[U];
         uint4 raw[U];
 #pragma unroll
@@ -1138,7 +1156,7 @@ __device__ __forceinline__ void stream_pass_tma(const CUtensorMap* tmap, int rb,
 // per team, as in the cp.async ring); `tmap` describes
 // X (columns [0, nvec * V), every row, one-row box).  TMA = false: the
 // per-thread cp.async ring of stream_pass (tmap unused).
-template <typename XT, typename YT, int TL, int VPL, int V, int S, int BLOCK, bool TMA = false>
+template <typename XT, typename YT, int TL, int VPL, int V, int S, int BLOCK, bool TMA = false, bool OFF32 = false>
 __global__ void __launch_bounds__(BLOCK) fwd_stream_kernel(const FwdArgs a, const __grid_constant__ CUtensorMap tmap) {
   extern __shared__ __align__(128) uint4 ring[];
   const int lane = threadIdx.x & 31;
@@ -1206,7 +1224,7 @@ __global__ void __launch_bounds__(BLOCK) fwd_stream_kernel(const FwdArgs a, cons
         stream_pass_tma<XT, TL, VPL, V, G>(&tmap, a.tma_rb, a.cent, a.cval, cb, clen, a.scale_mode, a.mult, tring, tbar,
                                         tphase, tl, tmask, next_end, on_end, ch_dv, hints, true, a.qs, a.timeout_ns);
       } else {
-        stream_pass<XT, TL, VPL, V, S, BLOCK>(x, a.ldx, a.nvec, a.cent, a.cval, cb, clen, a.scale_mode, a.mult,
+        stream_pass<XT, TL, VPL, V, S, BLOCK, OFF32>(x, a.ldx, a.nvec, a.cent, a.cval, cb, clen, a.scale_mode, a.mult,
                                               ring, tl, tmask, next_end, on_end, ch_dv, hints, true);
       }
     }
@@ -1400,7 +1418,7 @@ __global__ void __launch_bounds__(BLOCK) fwd_stream_kernel(const FwdArgs a, cons
                                         tphase, tl, tmask, next_end, on_end, row_dv, hints, lockstep, a.qs,
                                         a.timeout_ns);
       } else {
-        stream_pass<XT, TL, VPL, V, S, BLOCK>(x, a.ldx, a.nvec, a.ent, a.val, k0, len, a.scale_mode, a.mult, ring,
+        stream_pass<XT, TL, VPL, V, S, BLOCK, OFF32>(x, a.ldx, a.nvec, a.ent, a.val, k0, len, a.scale_mode, a.mult, ring,
                                               tl, tmask, next_end, on_end, row_dv, hints, lockstep);
       }
     }
@@ -1514,9 +1532,9 @@ __device__ __forceinline__ void gather_dual(float (&acc)[VPL][V], const GT* __re
           const int vi = tl + v * TL;
           if (j + u < cnt && vi < nvec) {
             if (in) {
-              load_f32_cg<V>(h + (int64_t)r * ldp + vi * V, buf[u][v]);
+              load_f32_cg<V>(h + row_off(r, ldp) + vi * V, buf[u][v]);
             } else {
-              Vec<GT, V>::load(g + (int64_t)r * ldg + (int64_t)vi * V, buf[u][v]);
+              Vec<GT, V>::load(g + row_off(r, ldg) + (int64_t)vi * V, buf[u][v]);
             }
           } else {
 #pragma unroll
@@ -1580,9 +1598,9 @@ __device__ __forceinline__ void gather_dual_split(float (&acc)[VPL][V], const GT
           const int vi = tl + v * TL;
           if (jj < cnt && vi < nvec) {
             if (in) {
-              load_f32_cg<V>(h + (int64_t)r * ldp + vi * V, buf[u][v]);
+              load_f32_cg<V>(h + row_off(r, ldp) + vi * V, buf[u][v]);
             } else {
-              Vec<GT, V>::load(g + (int64_t)r * ldg + (int64_t)vi * V, buf[u][v]);
+              Vec<GT, V>::load(g + row_off(r, ldg) + (int64_t)vi * V, buf[u][v]);
             }
           } else {
 #pragma unroll

@@ -58,7 +58,10 @@ int launch_fwd_t(cbm_plan* P, const FwdArgs& a, cudaStream_t st) {
 template <typename XT, typename YT, int TL, int VPL, int V, int S, bool TMA = false>
 int launch_stream_t(cbm_plan* P, const FwdArgs& a, const CUtensorMap& map, cudaStream_t st) {
   constexpr int n_teams = kStagedBlock / TL;
-  auto kern = fwd_stream_kernel<XT, YT, TL, VPL, V, S, kStagedBlock, TMA>;
+  // 32-bit X row offsets when every row offset of X fits them (X rows =
+  // the plan's columns)
+  const bool off32 = (uint64_t)P->n_cols * (uint64_t)a.ldx <= 0xffffffffull;
+  auto kern = fwd_stream_kernel<XT, YT, TL, VPL, V, S, kStagedBlock, TMA, false>;
   int grid;
   int smem;
   if constexpr (TMA) {
@@ -72,9 +75,10 @@ int launch_stream_t(cbm_plan* P, const FwdArgs& a, const CUtensorMap& map, cudaS
       per_sm = 1;
     grid = per_sm * sm_count(P->device);
   } else {
-    static GridCache cache;
+    static GridCache cache[2];
+    if (off32) kern = fwd_stream_kernel<XT, YT, TL, VPL, V, S, kStagedBlock, false, true>;
     smem = S * VPL * kStagedBlock * 16;
-    grid = cached_grid(cache, kern, P->device, kStagedBlock, smem);
+    grid = cached_grid(cache[off32 ? 1 : 0], kern, P->device, kStagedBlock, smem);
     if (grid <= 0) return CBM_ERR_CUDA;
   }
   kern<<<grid, kStagedBlock, smem, st>>>(a, map);

@@ -392,7 +392,7 @@ int matmul_impl(cbm_plan* P, int32_t op, float gin_scale, const void* x, int32_t
   if (!dtype_ok(xdt, ydt)) return CBM_ERR_DTYPE;
   if (n_cols == 0 || P->n_rows == 0) return CBM_OK;
   if (!x || !y) return CBM_ERR_INVALID;
-  if (ldx < n_cols || ldy < n_cols) return CBM_ERR_SHAPE;
+  if (ldx < n_cols || ldy < n_cols || ldx > INT32_MAX || ldy > INT32_MAX) return CBM_ERR_SHAPE;
   if (overlaps(x, extent(P->n_cols, ldx, n_cols, xdt), y, extent(P->n_rows, ldy, n_cols, ydt))) return CBM_ERR_SHAPE;
   // column multipliers (D[col]) need a square A; the ratio rule of the VALUES
   // op reads row multipliers only, so a rectangular plan (a row shard) may
@@ -642,7 +642,7 @@ int cbm_matmul_adjoint(cbm_plan* P, int32_t op, const void* g, int32_t gdt, int6
   if (!dtype_ok(gdt, ddt)) return CBM_ERR_DTYPE;
   if (n_cols == 0 || P->n_rows == 0 || P->n_cols == 0) return CBM_OK;
   if (!g || !dx) return CBM_ERR_INVALID;
-  if (ldg < n_cols || lddx < n_cols) return CBM_ERR_SHAPE;
+  if (ldg < n_cols || lddx < n_cols || ldg > INT32_MAX || lddx > INT32_MAX) return CBM_ERR_SHAPE;
   if (overlaps(g, extent(P->n_rows, ldg, n_cols, gdt), dx, extent(P->n_cols, lddx, n_cols, ddt))) return CBM_ERR_SHAPE;
   if ((op == CBM_OP_ADX || op == CBM_OP_DADX) && (!P->d_mult || P->n_rows != P->n_cols)) return CBM_ERR_UNSUPPORTED;
   cudaStream_t st = static_cast<cudaStream_t>(stream);

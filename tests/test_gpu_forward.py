@@ -405,3 +405,32 @@ def test_two_pass_equals_fused_on_a_deep_tree(op, cols):
         assert np.array_equal(ys["auto"], ys["fused"])
         np.testing.assert_array_equal(ys["two"], _oracle(op, a, x.float()))
     a.plan.check_device()
+
+
+@pytest.mark.parametrize("variant", ["staged", "register"])
+@pytest.mark.parametrize("dtype", [torch.bfloat16, torch.float32])
+def test_row_offsets_past_32_bits(variant, dtype):
+    """An X view whose row offsets pass 2^32 elements (leading dimension
+    2,100,000 over 2,100 rows) takes the kernels' 64-bit row addressing; the
+    product equals, bit for bit, the one on a compact copy of X (32-bit row
+    offsets) and the oracle's."""
+    dev = _dev()
+    n, cols, ld = 2100, 128, 2_100_000
+    assert (n - 1) * ld + cols > 2 ** 32
+    a = _make("ax", near_dup_graph(n, seed=12))
+    a.plan.tune(variant=variant)
+    # 8.8 GB (BF16) or 17.6 GB (FP32); only the view's n rows are written
+    buf = torch.empty((n - 1) * ld + cols, dtype=dtype, device=dev)
+    xv = buf.as_strided((n, cols), (ld, 1))
+    xc = torch.randn(n, cols, device=dev).to(dtype)
+    xv.copy_(xc)
+    y_wide = torch.empty(n, cols, device=dev)
+    y_compact = torch.empty_like(y_wide)
+    a.matmul(xv, y_wide)
+    a.matmul(xc, y_compact)
+    torch.cuda.synchronize()
+    del xv, buf
+    torch.cuda.empty_cache()
+    assert torch.equal(y_wide, y_compact)
+    np.testing.assert_array_equal(y_compact.cpu().numpy(), _oracle("ax", a, xc.float()))
+    a.plan.check_device()
