@@ -482,7 +482,7 @@ def _time_events(fn, steps, warmup):
 
 BATCH_SPACE = {"chunk_nnz": [128, 256], "rows_per_claim": [2, 4, 8], "variant": ["auto", "register"], "team": [0, 8]}
 PREC_SPACE = {"chunk_nnz": [256, 512], "rows_per_claim": [4, 8, 16], "variant": ["auto", "register", "tma"],
-              "hot_rows": [65536, 262144]}
+              "hot_rows": [0, 65536, 262144]}
 
 
 def batch_form(steps, warmup, space=None):
@@ -945,7 +945,8 @@ def main():
             torch.cuda.empty_cache()
             line["precision"] = _form(lambda: precision_form(max(args.steps, 10), args.warmup,
                                                              space={"chunk_nnz": [256, 512],
-                                                                    "rows_per_claim": [8, 16]}))
+                                                                    "rows_per_claim": [8, 16],
+                                                                    "hot_rows": [0, 65536]}))
             torch.cuda.empty_cache()
             line["batch"] = _form(lambda: batch_form(max(args.steps, 10), args.warmup))
             line["small"] = _form(lambda: small_form(max(args.steps, 10), max(args.warmup, 3)))

@@ -727,6 +727,11 @@ __device__ __forceinline__ void cp_async16_hint_n(void* smem, const void* gmem, 
                "l"(policy)
                : "memory");
 }
+// the same without an L2 policy
+__device__ __forceinline__ void cp_async16_n(void* smem, const void* gmem, unsigned bytes) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(s), "l"(gmem), "r"(bytes) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
@@ -820,7 +825,8 @@ __device__ __forceinline__ float entry_scale(uint32_t e, int64_t idx, bool valid
 // current item ends (INT_MAX when none is left); on_end(acc) finishes it,
 // resets acc and advances, updating row_dv (the row factor: m[row] under
 // SCALE_DCOL_DROW, exactly 1 otherwise).
-template <typename XT, int TL, int VPL, int V, int S, int BLOCK, bool OFF32, typename NextEnd, typename OnEnd>
+template <typename XT, int TL, int VPL, int V, int S, int BLOCK, bool OFF32, bool HINTS, typename NextEnd,
+          typename OnEnd>
 __device__ __forceinline__ void stream_pass(const XT* __restrict__ x, int64_t ldx, int nvec,
                                             const uint32_t* __restrict__ ent, const float* __restrict__ val,
                                             int64_t k0, int len, int scale_mode, const float* __restrict__ mult,
@@ -875,20 +881,33 @@ __device__ __forceinline__ void stream_pass(const XT* __restrict__ x, int64_t ld
   // are skipped (the slots keep old data, never read).
   const XT* xp = piece_ok[0] ? xl : x;
   auto produce = [&](int p, uint4* sp) {
+    // HINTS: the entry's hot bit picks its L2 policy; without (a plan with
+    // no hot set) the copies carry no policy and need no per-entry choice
     if constexpr (VPL == 1) {
       const bool inA = p < bA + TL;
       const uint32_t e = __shfl_sync(tmask, inA ? eA : eB, p & (TL - 1), TL);
       const XT* row = row_at(xp, e);
-      const uint64_t pol = (e & kHotBit) ? pol_keep : pol_stream;
-      cp_async16_hint_n(sp, row, p < len ? 16u : 0u, pol);
+      if constexpr (HINTS) {
+        const uint64_t pol = (e & kHotBit) ? pol_keep : pol_stream;
+        cp_async16_hint_n(sp, row, p < len ? 16u : 0u, pol);
+      } else {
+        cp_async16_n(sp, row, p < len ? 16u : 0u);
+      }
     } else if (p < len) {
       const bool inA = p < bA + TL;
       const uint32_t e = __shfl_sync(tmask, inA ? eA : eB, p & (TL - 1), TL);
       const XT* row = row_at(xl, e);
       const uint64_t pol = (e & kHotBit) ? pol_keep : pol_stream;
 #pragma unroll
-      for (int v = 0; v < VPL; ++v)
-        if (piece_ok[v]) cp_async16_hint(sp + v * BLOCK, row + v * TL * V, pol);
+      for (int v = 0; v < VPL; ++v) {
+        if (piece_ok[v]) {
+          if constexpr (HINTS) {
+            cp_async16_hint(sp + v * BLOCK, row + v * TL * V, pol);
+          } else {
+            cp_async16(sp + v * BLOCK, row + v * TL * V);
+          }
+        }
+      }
     }
   };
   // Entries move in groups of U (one cp.async group each, S / U groups in
@@ -1156,7 +1175,8 @@ __device__ __forceinline__ void stream_pass_tma(const CUtensorMap* tmap, int rb,
 // per team, as in the cp.async ring); `tmap` describes
 // X (columns [0, nvec * V), every row, one-row box).  TMA = false: the
 // per-thread cp.async ring of stream_pass (tmap unused).
-template <typename XT, typename YT, int TL, int VPL, int V, int S, int BLOCK, bool TMA = false, bool OFF32 = false>
+template <typename XT, typename YT, int TL, int VPL, int V, int S, int BLOCK, bool TMA = false, bool OFF32 = false,
+          bool HINTS = true>
 __global__ void __launch_bounds__(BLOCK) fwd_stream_kernel(const FwdArgs a, const __grid_constant__ CUtensorMap tmap) {
   extern __shared__ __align__(128) uint4 ring[];
   const int lane = threadIdx.x & 31;
@@ -1224,7 +1244,7 @@ __global__ void __launch_bounds__(BLOCK) fwd_stream_kernel(const FwdArgs a, cons
         stream_pass_tma<XT, TL, VPL, V, G>(&tmap, a.tma_rb, a.cent, a.cval, cb, clen, a.scale_mode, a.mult, tring, tbar,
                                         tphase, tl, tmask, next_end, on_end, ch_dv, hints, true, a.qs, a.timeout_ns);
       } else {
-        stream_pass<XT, TL, VPL, V, S, BLOCK, OFF32>(x, a.ldx, a.nvec, a.cent, a.cval, cb, clen, a.scale_mode, a.mult,
+        stream_pass<XT, TL, VPL, V, S, BLOCK, OFF32, HINTS>(x, a.ldx, a.nvec, a.cent, a.cval, cb, clen, a.scale_mode, a.mult,
                                               ring, tl, tmask, next_end, on_end, ch_dv, hints, true);
       }
     }
@@ -1418,7 +1438,7 @@ __global__ void __launch_bounds__(BLOCK) fwd_stream_kernel(const FwdArgs a, cons
                                         tphase, tl, tmask, next_end, on_end, row_dv, hints, lockstep, a.qs,
                                         a.timeout_ns);
       } else {
-        stream_pass<XT, TL, VPL, V, S, BLOCK, OFF32>(x, a.ldx, a.nvec, a.ent, a.val, k0, len, a.scale_mode, a.mult, ring,
+        stream_pass<XT, TL, VPL, V, S, BLOCK, OFF32, HINTS>(x, a.ldx, a.nvec, a.ent, a.val, k0, len, a.scale_mode, a.mult, ring,
                                               tl, tmask, next_end, on_end, row_dv, hints, lockstep);
       }
     }

@@ -75,10 +75,14 @@ int launch_stream_t(cbm_plan* P, const FwdArgs& a, const CUtensorMap& map, cudaS
       per_sm = 1;
     grid = per_sm * sm_count(P->device);
   } else {
-    static GridCache cache[2];
-    if (off32) kern = fwd_stream_kernel<XT, YT, TL, VPL, V, S, kStagedBlock, false, true>;
+    // a plan without a hot set (hints off) takes copies without L2 policies
+    // (the 64-bit form keeps the policy kernel: policies are then all normal)
+    static GridCache cache[3];
+    const int form = !off32 ? 0 : a.hints ? 1 : 2;
+    if (form == 1) kern = fwd_stream_kernel<XT, YT, TL, VPL, V, S, kStagedBlock, false, true, true>;
+    if (form == 2) kern = fwd_stream_kernel<XT, YT, TL, VPL, V, S, kStagedBlock, false, true, false>;
     smem = S * VPL * kStagedBlock * 16;
-    grid = cached_grid(cache[off32 ? 1 : 0], kern, P->device, kStagedBlock, smem);
+    grid = cached_grid(cache[form], kern, P->device, kStagedBlock, smem);
     if (grid <= 0) return CBM_ERR_CUDA;
   }
   kern<<<grid, kStagedBlock, smem, st>>>(a, map);

@@ -349,13 +349,15 @@ def test_bounded_wait_times_out_and_recovers(passes):
 @pytest.mark.parametrize("team", [8, 16, 32])
 @pytest.mark.parametrize("cols,dtype", [(256, torch.float32), (64, torch.float32), (128, torch.bfloat16),
                                         (512, torch.float32)])
-def test_staged_team_shapes(team, cols, dtype):
+@pytest.mark.parametrize("hot_rows", [65536, 0])
+def test_staged_team_shapes(team, cols, dtype, hot_rows):
     """Every team size of the staged kernel (several row streams per warp stepping
-    together) gives the oracle's result bit for bit on unsplit rows."""
+    together) gives the oracle's result bit for bit on unsplit rows, with L2
+    policies per entry (a hot set) and without (hot_rows 0)."""
     dev = _dev()
     ei = near_dup_graph(3000, seed=23, deg=14)
     a = _make("dadx", ei)
-    a.plan.tune(variant="staged", team=team, rows_per_claim=3)
+    a.plan.tune(variant="staged", team=team, rows_per_claim=3, hot_rows=hot_rows)
     x = torch.randn(3000, cols, device=dev).to(dtype)
     y = torch.empty(3000, cols, device=dev)
     a.matmul(x, y)
