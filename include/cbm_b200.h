@@ -46,7 +46,7 @@ enum {
   CBM_ERR_CUDA = 4,        /* a CUDA runtime call failed */
   CBM_ERR_STRUCTURE = 5,   /* not a forest / duplicate child / bad offsets */
   CBM_ERR_DTYPE = 6,       /* unsupported dtype combination */
-  CBM_ERR_SHAPE = 7,       /* leading dimension < columns, aliasing x and y */
+  CBM_ERR_SHAPE = 7,       /* leading dimension < columns or >= 2^31, aliasing x and y */
   CBM_ERR_TIMEOUT = 8,     /* a device wait ran out (see cbm_plan_error) */
   CBM_ERR_UNSUPPORTED = 9, /* op needs multipliers / values the plan lacks */
   CBM_ERR_WORKSPACE = 10,  /* workspace smaller than cbm_plan_workspace_bytes */
