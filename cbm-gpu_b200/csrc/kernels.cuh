@@ -284,8 +284,9 @@ __host__ __device__ constexpr int unroll_for() {
 }
 
 // acc += sum over entries [beg, end) of scale_k * X[col_k], UF entries' gathers
-// in flight per lane (0: unroll_for's choice)
-template <typename XT, int VPL, int V, int UF = 0>
+// in flight per lane (0: unroll_for's choice); OFF32: X holds fewer than 2^32
+// elements, so a row's offset is 32-bit element arithmetic
+template <typename XT, int VPL, int V, int UF = 0, bool OFF32 = false>
 __device__ __forceinline__ void gather_range(float (&acc)[VPL][V], const XT* __restrict__ x, int64_t ldx, int nvec,
                                              const uint32_t* __restrict__ ent, const float* __restrict__ val,
                                              int64_t beg, int64_t end, int scale_mode,
@@ -318,7 +319,7 @@ __device__ __forceinline__ void gather_range(float (&acc)[VPL][V], const XT* __r
       for (int u = 0; u < U; ++u) {
         const uint32_t eu = __shfl_sync(tmask, e, j + u < cnt ? j + u : 0, TL);
         s[u] = __shfl_sync(tmask, sc, j + u < cnt ? j + u : 0, TL);
-        const XT* row = x + row_off(eu & kColMask, ldx);
+        const XT* row = OFF32 ? x + (uint32_t)((eu & kColMask) * (uint32_t)ldx) : x + row_off(eu & kColMask, ldx);
 #pragma unroll
         for (int v = 0; v < VPL; ++v) {
           const int vi = tl + v * TL;
@@ -364,7 +365,7 @@ __host__ __device__ constexpr int fwd_in_flight() {
   return fwd_min_blocks<XT, YT, VPL, COMP, WIDE>() == 4 ? 2 : 0;  // 0: unroll_for's choice
 }
 
-template <typename XT, typename YT, int VPL, int V, bool COMP = false, bool WIDE = false>
+template <typename XT, typename YT, int VPL, int V, bool COMP = false, bool WIDE = false, bool OFF32 = false>
 __device__ __forceinline__ void fwd_chunk(const FwdArgs& a, int k, unsigned epoch, int tl, int TL, unsigned tmask) {
   float acc[VPL][V];
 #pragma unroll
@@ -374,7 +375,7 @@ __device__ __forceinline__ void fwd_chunk(const FwdArgs& a, int k, unsigned epoc
   const int item = a.chunk_item[k];
   const int node = a.node[item] & 0x7fffffff;
   const float dv = (a.scale_mode == SCALE_DCOL_DROW) ? __ldg(a.mult + node) : 1.f;
-  gather_range<XT, VPL, V, fwd_in_flight<XT, YT, VPL, COMP, WIDE>()>(
+  gather_range<XT, VPL, V, fwd_in_flight<XT, YT, VPL, COMP, WIDE>(), OFF32>(
       acc, static_cast<const XT*>(a.x), a.ldx, a.nvec, a.cent, a.cval, a.chunk_beg[k], a.chunk_end[k],
       a.scale_mode, a.mult, dv, tl, TL, tmask);
   float* prow = a.partial + (int64_t)k * a.ldp;
@@ -409,7 +410,7 @@ __device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
   e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bp)), __fsub_rn(b, bp));
 }
 
-template <typename XT, typename YT, int VPL, int V, bool COMP = false, bool WIDE = false>
+template <typename XT, typename YT, int VPL, int V, bool COMP = false, bool WIDE = false, bool OFF32 = false>
 __device__ __forceinline__ void fwd_row(const FwdArgs& a, int item, unsigned epoch, int tl, int TL, unsigned tmask) {
   float acc[VPL][V];
 #pragma unroll
@@ -423,7 +424,7 @@ __device__ __forceinline__ void fwd_row(const FwdArgs& a, int item, unsigned epo
   const float dv = need_dv ? __ldg(a.mult + node) : 1.f;
   const int c0 = a.chunk0[item];
   if (c0 < 0) {
-    gather_range<XT, VPL, V, fwd_in_flight<XT, YT, VPL, COMP, WIDE>()>(
+    gather_range<XT, VPL, V, fwd_in_flight<XT, YT, VPL, COMP, WIDE>(), OFF32>(
         acc, static_cast<const XT*>(a.x), a.ldx, a.nvec, a.ent, a.val, a.ptr[item], a.ptr[item + 1],
         a.scale_mode, a.mult, dv, tl, TL, tmask);
   } else {
@@ -563,7 +564,7 @@ __device__ __forceinline__ void finish_block(QueueState* qs, unsigned epoch, boo
   }
 }
 
-template <typename XT, typename YT, int VPL, int V, bool COMP = false, bool WIDE = false>
+template <typename XT, typename YT, int VPL, int V, bool COMP = false, bool WIDE = false, bool OFF32 = false>
 __global__ void __launch_bounds__(kThreads, (fwd_min_blocks<XT, YT, VPL, COMP, WIDE>()))
     fwd_kernel(const FwdArgs a) {
   const int lane = threadIdx.x & 31;
@@ -581,7 +582,7 @@ __global__ void __launch_bounds__(kThreads, (fwd_min_blocks<XT, YT, VPL, COMP, W
       base = __shfl_sync(0xffffffffu, base, 0);
       if (base >= (unsigned)a.n_chunks) break;
       const unsigned k = base + team;
-      if (k < (unsigned)a.n_chunks) fwd_chunk<XT, YT, VPL, V, COMP, WIDE>(a, (int)k, epoch, tl, TL, tmask);
+      if (k < (unsigned)a.n_chunks) fwd_chunk<XT, YT, VPL, V, COMP, WIDE, OFF32>(a, (int)k, epoch, tl, TL, tmask);
       __syncwarp();
     }
   }
@@ -598,7 +599,7 @@ __global__ void __launch_bounds__(kThreads, (fwd_min_blocks<XT, YT, VPL, COMP, W
     for (int r = 0; r < R; ++r) {
       const unsigned item = base + team + (unsigned)(r * teams);
       if (item >= (unsigned)a.n_items) break;
-      fwd_row<XT, YT, VPL, V, COMP, WIDE>(a, (int)item, epoch, tl, TL, tmask);
+      fwd_row<XT, YT, VPL, V, COMP, WIDE, OFF32>(a, (int)item, epoch, tl, TL, tmask);
     }
     __syncwarp();
   }

@@ -45,9 +45,16 @@ int cached_grid(GridCache& c, K kernel, int device, int block, int smem) {
 
 template <typename XT, typename YT, int VPL, int V, bool COMP = false, bool WIDE = false>
 int launch_fwd_t(cbm_plan* P, const FwdArgs& a, cudaStream_t st) {
-  static GridCache cache;
-  auto kern = fwd_kernel<XT, YT, VPL, V, COMP, WIDE>;
-  const int grid = cached_grid(cache, kern, P->device, kThreads, 0);
+  static GridCache cache[2];
+  // BF16 X with fewer than 2^32 elements takes 32-bit row offsets (measured
+  // faster there; FP32 X keeps the widening multiply)
+  bool off32 = false;
+  auto kern = fwd_kernel<XT, YT, VPL, V, COMP, WIDE, false>;
+  if constexpr (sizeof(XT) == 2) {
+    off32 = (uint64_t)P->n_cols * (uint64_t)a.ldx <= 0xffffffffull;
+    if (off32) kern = fwd_kernel<XT, YT, VPL, V, COMP, WIDE, true>;
+  }
+  const int grid = cached_grid(cache[off32 ? 1 : 0], kern, P->device, kThreads, 0);
   if (grid <= 0) return CBM_ERR_CUDA;
   kern<<<grid, kThreads, 0, st>>>(a);
   P->launches++;
