@@ -55,6 +55,7 @@ SIGNATURES = [
     ("cbm_plan_set_timeout", C.c_int, [vp, i64]),
     ("cbm_plan_set_passes", C.c_int, [vp, i32]),
     ("cbm_plan_set_host_overlap", C.c_int, [vp, i32]),
+    ("cbm_plan_host_wait", C.c_int, [vp, vp]),
     ("cbm_plan_set_compensation", C.c_int, [vp, i32]),
     ("cbm_plan_debug_set_parent", C.c_int, [vp, i64, i32, vp]),
     ("cbm_plan_debug_check_transpose", C.c_int, [vp, vp]),

@@ -69,9 +69,16 @@ class cbm4mm:  # noqa: N801 (the reference's class name)
         """y <- (this operator) x for host tensors x and y (pinned for full-speed
         copies), the copies overlapped with the product slab by slab.  Queued on
         the current stream: synchronise it before reading y.  overlap_calls:
-        back-to-back calls also overlap one call's last copy-out with the next
-        call's first copy-in (x must be complete in host memory at the call)."""
+        back-to-back calls also overlap one call's copy-out with the next
+        call's copy-in (x must be complete in host memory at the call), and the
+        current stream waits only for the products: call host_wait() before
+        synchronising to read y."""
         self._plan.matmul_host(self._op, x, y, slab_cols, overlap_calls)
+
+    def host_wait(self):
+        """The current stream waits for every copy-out of matmul_host calls so
+        far (after calls with overlap_calls)."""
+        self._plan.host_wait()
 
     @property
     def self_adjoint(self):

@@ -194,9 +194,10 @@ class Plan:
         streams.  Device buffers of the operand shapes are allocated on the first
         call and reused.  Returns once queued; the current stream waits for the
         last copy (synchronise it before reading y).  overlap_calls: this call's
-        copy-in may run under the previous call's last copy-out (x must then be
-        complete in host memory when the call is made; see
-        cbm_plan_set_host_overlap)."""
+        copy-in may run under the previous call's copy-out (x must then be
+        complete in host memory when the call is made), and the current stream
+        waits only for this call's products: call host_wait() before
+        synchronising to read y (see cbm_plan_set_host_overlap)."""
         op = OPS[op] if isinstance(op, str) else int(op)
         for t, rows, name in ((x, self.n_cols, "rhs"), (y, self.n_rows, "res")):
             if not isinstance(t, torch.Tensor) or t.is_cuda:
@@ -224,6 +225,11 @@ class Plan:
                                        ydt, max(int(y.stride(0)), cols, 1), cols, int(slab_cols), xd.data_ptr(),
                                        yd.data_ptr(), ws.data_ptr(), ws.numel(), _stream(self.device))
         _lib.check(rc, "cbm_matmul_host")
+
+    def host_wait(self):
+        """The current stream waits for every copy-out of matmul_host calls
+        made so far (needed after overlap_calls before y is read)."""
+        _lib.check(self._lib.cbm_plan_host_wait(self._h, _stream(self.device)), "cbm_plan_host_wait")
 
     def adjoint(self, op, g, dx):
         """dx <- op(A)^T g on the current stream."""

@@ -288,6 +288,7 @@ void release_pipeline(cbm_plan* P) {
   if (P->host_prev_prod) cudaEventDestroy(P->host_prev_prod);
   P->host_prev_prod = nullptr;
   P->host_prev_valid = false;
+  P->host_out_pending = false;
   if (P->h2d) cudaStreamDestroy(P->h2d);
   if (P->d2h) cudaStreamDestroy(P->d2h);
   P->h2d = P->d2h = nullptr;
@@ -588,46 +589,72 @@ int cbm_matmul_host(cbm_plan* P, int32_t op, const void* x_host, int32_t xdt, in
   const int64_t n_slabs = (int64_t)bounds.size() - 1;
   if (n_slabs > 4096) return CBM_ERR_INVALID;
   // the product's own checks (workspace, multipliers, op) run on the first slab
-  int rc = pipeline_ready(P, (size_t)(2 * n_slabs + 2));
+  int rc = pipeline_ready(P, (size_t)(3 * n_slabs + 2));
   if (rc) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   cudaEvent_t* ev = P->events.data();
-  // the copy streams start after the work already queued on the caller's
-  // stream; with overlap across calls, the copy-in waits only until the
-  // previous call's products no longer read the device copy of X (so it runs
-  // under that call's last copy-out)
+  const bool overlap = P->host_overlap;
+  const int64_t layout[5] = {n_cols, w, n_slabs, xs, ys};
+  const bool same_layout = P->host_prev_valid && std::equal(layout, layout + 5, P->host_prev_layout) &&
+                           P->host_prev_xd == x_dev && P->host_prev_yd == y_dev;
+  // the copy-out stream starts after the work already queued on the caller's
+  // stream.  The copy-in does too, except with overlap after a previous call:
+  // then it waits only until that call's products no longer read the device
+  // copy of X (slab by slab with the same layout), so it runs under that
+  // call's copy-out
   if (cudaEventRecord(ev[0], st) != cudaSuccess) return CBM_ERR_CUDA;
-  const bool overlap = P->host_overlap && P->host_prev_valid;
-  if (cudaStreamWaitEvent(P->h2d, overlap ? P->host_prev_prod : ev[0], 0) != cudaSuccess) return CBM_ERR_CUDA;
   if (cudaStreamWaitEvent(P->d2h, ev[0], 0) != cudaSuccess) return CBM_ERR_CUDA;
+  if (!(overlap && P->host_prev_valid)) {
+    if (cudaStreamWaitEvent(P->h2d, ev[0], 0) != cudaSuccess) return CBM_ERR_CUDA;
+  } else if (!same_layout) {
+    if (cudaStreamWaitEvent(P->h2d, P->host_prev_prod, 0) != cudaSuccess) return CBM_ERR_CUDA;
+  }
+  // a previous call's copy-out still pending: the products may not overwrite
+  // the device copy of Y before it has left (slab by slab with the same layout)
+  const bool wait_out = P->host_prev_valid && P->host_out_pending;
+  if (wait_out && !same_layout && cudaStreamWaitEvent(st, ev[1], 0) != cudaSuccess) return CBM_ERR_CUDA;
   const char* xh = static_cast<const char*>(x_host);
   char* yh = static_cast<char*>(y_host);
   char* xd = static_cast<char*>(x_dev);
   char* yd = static_cast<char*>(y_dev);
   for (int64_t k = 0; k < n_slabs; ++k) {
     const int64_t c0 = bounds[k], cw = bounds[k + 1] - c0;
-    cudaEvent_t in = ev[2 + 2 * k], out = ev[3 + 2 * k];
+    cudaEvent_t in = ev[2 + 3 * k], prod = ev[3 + 3 * k], out = ev[4 + 3 * k];
+    // each wait on the previous call's event of slab k is queued before this
+    // call records that event again
+    if (overlap && same_layout && cudaStreamWaitEvent(P->h2d, prod, 0) != cudaSuccess) return CBM_ERR_CUDA;
     if (cudaMemcpy2DAsync(xd + c0 * xs, n_cols * xs, xh + c0 * xs, ldx_host * xs, cw * xs, P->n_cols,
                           cudaMemcpyHostToDevice, P->h2d) != cudaSuccess)
       return CBM_ERR_CUDA;
     if (cudaEventRecord(in, P->h2d) != cudaSuccess) return CBM_ERR_CUDA;
     if (cudaStreamWaitEvent(st, in, 0) != cudaSuccess) return CBM_ERR_CUDA;
+    if (wait_out && same_layout && cudaStreamWaitEvent(st, out, 0) != cudaSuccess) return CBM_ERR_CUDA;
     rc = cbm_matmul(P, op, xd + c0 * xs, xdt, n_cols, yd + c0 * ys, ydt, n_cols, cw, ws, ws_bytes, stream);
     if (rc) return rc;
-    if (cudaEventRecord(out, st) != cudaSuccess) return CBM_ERR_CUDA;
-    if (k + 1 == n_slabs) {
-      if (cudaEventRecord(P->host_prev_prod, st) != cudaSuccess) return CBM_ERR_CUDA;
-      P->host_prev_valid = true;
-    }
-    if (cudaStreamWaitEvent(P->d2h, out, 0) != cudaSuccess) return CBM_ERR_CUDA;
+    if (cudaEventRecord(prod, st) != cudaSuccess) return CBM_ERR_CUDA;
+    if (k + 1 == n_slabs && cudaEventRecord(P->host_prev_prod, st) != cudaSuccess) return CBM_ERR_CUDA;
+    if (cudaStreamWaitEvent(P->d2h, prod, 0) != cudaSuccess) return CBM_ERR_CUDA;
     if (cudaMemcpy2DAsync(yh + c0 * ys, ldy_host * ys, yd + c0 * ys, n_cols * ys, cw * ys, P->n_rows,
                           cudaMemcpyDeviceToHost, P->d2h) != cudaSuccess)
       return CBM_ERR_CUDA;
+    if (cudaEventRecord(out, P->d2h) != cudaSuccess) return CBM_ERR_CUDA;
   }
-  // the caller's stream resumes once the last slab is back in host memory
   if (cudaEventRecord(ev[1], P->d2h) != cudaSuccess) return CBM_ERR_CUDA;
-  if (cudaStreamWaitEvent(st, ev[1], 0) != cudaSuccess) return CBM_ERR_CUDA;
+  P->host_prev_valid = true;
+  std::copy(layout, layout + 5, P->host_prev_layout);
+  P->host_prev_xd = x_dev;
+  P->host_prev_yd = y_dev;
+  // without overlap the caller's stream resumes once the last slab is back in
+  // host memory; with it, once the products are done (the copy-out pending)
+  P->host_out_pending = overlap;
+  if (!overlap && cudaStreamWaitEvent(st, ev[1], 0) != cudaSuccess) return CBM_ERR_CUDA;
   return CBM_OK;
+}
+
+int cbm_plan_host_wait(cbm_plan* P, void* stream) {
+  if (!P) return CBM_ERR_INVALID;
+  if (!P->host_out_pending || P->events.size() < 2) return CBM_OK;
+  return cuda_status(cudaStreamWaitEvent(static_cast<cudaStream_t>(stream), P->events[1], 0));
 }
 
 int cbm_plan_prepare_adjoint(cbm_plan* P, void* stream) {

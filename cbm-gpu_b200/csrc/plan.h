@@ -103,12 +103,23 @@ struct cbm_plan {
   // that order slabs across them, created on first use
   cudaStream_t h2d = nullptr, d2h = nullptr;
   std::vector<cudaEvent_t> events;
-  // overlap across calls (cbm_plan_set_host_overlap): the copy-in of a call
-  // waits only for the previous call's last product (recorded in
-  // host_prev_prod), not for its copy-out
+  // overlap across calls (cbm_plan_set_host_overlap).  Events per slab k:
+  // events[2 + 3k] copy-in done, [3 + 3k] product done, [4 + 3k] copy-out
+  // done; [0] the call's start on the caller's stream, [1] its last copy-out.
+  // A call with the previous call's slab layout orders slab by slab against
+  // it (its copy-in of slab k after that call's product k, its product k
+  // after that call's copy-out k); otherwise against the whole call
+  // (host_prev_prod: the last product; events[1]: the last copy-out).  With
+  // overlap the caller's stream is released after the products and the
+  // copy-out stays pending (host_out_pending) until cbm_plan_host_wait or a
+  // call without overlap.
   bool host_overlap = false;
   bool host_prev_valid = false;
+  bool host_out_pending = false;
   cudaEvent_t host_prev_prod = nullptr;
+  int64_t host_prev_layout[5] = {0, 0, 0, 0, 0};  // columns, slab width, slabs, x and y element bytes
+  const void* host_prev_xd = nullptr;
+  const void* host_prev_yd = nullptr;
 };
 
 namespace cbm {

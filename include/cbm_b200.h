@@ -226,15 +226,25 @@ int cbm_matmul_host(cbm_plan* plan, int32_t op, const void* x_host, int32_t x_dt
                     void* y_host, int32_t y_dtype, int64_t ldy_host, int64_t n_cols, int64_t slab_cols,
                     void* x_dev, void* y_dev, void* workspace, int64_t workspace_bytes, void* stream);
 
-/* cbm_matmul_host across calls (0: off, the default): with it on, a call's
- * copy-in of X waits only until the previous call's products have finished
- * reading the device copy of X, not for the previous call's copy-out, so
- * back-to-back calls overlap one's last copy-out with the next one's first
- * copy-in.  The copy-in is then not ordered after other work the caller
- * queued on `stream`: x_host must be complete when the call is made (written
- * by the host).  Results and the end-of-call guarantee (a synchronisation of
- * `stream` makes y_host final) are unchanged. */
+/* cbm_matmul_host across calls (0: off, the default).  With it on:
+ *  - a call's copy-in of X waits only until the previous call's products have
+ *    finished reading the device copy of X (slab by slab when both calls
+ *    have the same columns, slab width, dtypes and device buffers), not for
+ *    the previous call's copy-out, so copies in and out of consecutive calls
+ *    overlap.  The copy-in is not ordered after other work the caller queued
+ *    on `stream`: x_host must be complete when the call is made (written by
+ *    the host);
+ *  - `stream` waits for the call's products only: its copy-out of Y stays
+ *    pending.  cbm_plan_host_wait(plan, stream) makes `stream` wait for every
+ *    copy-out queued so far; after that a synchronisation of `stream` makes
+ *    y_host final.  A call without overlap also ends with `stream` waiting
+ *    for every copy-out, as before.
+ * Results are unchanged. */
 int cbm_plan_set_host_overlap(cbm_plan* plan, int32_t on);
+
+/* `stream` waits for every copy-out of Y queued by cbm_matmul_host calls of
+ * this plan (needed after calls with overlap on; no effect otherwise). */
+int cbm_plan_host_wait(cbm_plan* plan, void* stream);
 
 /* dX = op(A)^T G (the adjoint of cbm_matmul for CBM_OP_AX/ADX/DADX): a
  * reverse tree propagation (children into parents) then a transposed delta

@@ -78,3 +78,24 @@ def test_back_to_back_calls_with_overlap(op_dad, slab):
     op_dad.matmul(xs[0].cuda(), ref)
     assert torch.equal(last, ref.cpu())
     op_dad.plan.check_device()
+
+
+@pytest.mark.parametrize("slab", [64, 96])
+def test_overlapped_calls_released_before_copy_out(op_dad, slab):
+    """With overlap_calls the current stream waits only for the products: the
+    copy-outs finish after host_wait().  Four calls with the same slab layout
+    (ordered slab by slab), then one with another slab width (ordered against
+    the whole previous call), each equal to the device product."""
+    n = op_dad.num_nodes
+    g = torch.Generator().manual_seed(100 + slab)
+    xs = [torch.randn(n, 192, generator=g).pin_memory() for _ in range(5)]
+    ys = [torch.full((n, 192), float("nan")).pin_memory() for _ in range(5)]
+    for i, (x, y) in enumerate(zip(xs, ys)):
+        op_dad.matmul_host(x, y, slab_cols=slab if i < 4 else 128, overlap_calls=True)
+    op_dad.host_wait()
+    torch.cuda.current_stream().synchronize()
+    ref = torch.empty(n, 192, device="cuda")
+    for x, y in zip(xs, ys):
+        op_dad.matmul(x.cuda(), ref)
+        assert torch.equal(y, ref.cpu())
+    op_dad.plan.check_device()
