@@ -17,9 +17,11 @@ plain FP32, and their ratio (rank 0 only).
 At N = 1 the line also carries the other forms, each measured on the device
 with CUDA events after its own warm-up, outside the headline's timed region:
 "precision" (A D^-1/2 X on the 2.4M-node workload, X stored BF16), "batch"
-(the 512-graph workload in one launch replayed from a CUDA graph) and "small"
+(the 512-graph workload in one launch replayed from a CUDA graph), "small"
 (A.X on the 4,096-node community graph: launch latency, eager and from a CUDA
-graph), with error against FP64 on sampled rows.
+graph) and "direct" (the reference's operator s_spmm_fused_update_csr_int32
+through its own signature on CUDA tensors, on the headline's structure), with
+error against FP64 on sampled rows.
 
 N > 1 runs under torchrun, one rank per GPU: each rank owns a 256-column shard
 of X and Y (column sharding needs no collective; weak scaling).  Rank 0
@@ -599,6 +601,37 @@ def run_precision(args):
     print(json.dumps(line), flush=True)
 
 
+def direct_form(a, x, y_plan, b_alg, plan_ms, steps, warmup):
+    """The reference's CPU operator s_spmm_fused_update_csr_int32
+    (cbm/cbm_extensions.cpp:593-698) through its own signature on CUDA tensors
+    (csrc/direct.cu: no plan; the caller's CSR and tree arrays read as given),
+    on the headline's structure, prepared values, multipliers and X: ms per
+    product at the headline's algorithmic bytes, beside the plan path, and its
+    agreement with the plan path's result (rtol 1e-5, atol 1e-6: its update
+    rounds as the CPU code does, fma(Y[u], m[v] / m[u], Y[v]))."""
+    from cbm import cbm_mkl_cpp
+
+    crow = a.deltas.crow_indices()
+    rp_b, rp_e = crow[:-1], crow[1:]
+    col, val = a.deltas.col_indices(), a.deltas.values()
+    out = torch.empty_like(y_plan)
+
+    def run():
+        cbm_mkl_cpp.s_spmm_fused_update_csr_int32(rp_b, rp_e, col, val, x, a.mca_offset, a.mca_src_idx,
+                                                  a.mca_dst_idx, a.D, out)
+
+    ms = _time_events(run, steps, warmup)
+    run()
+    torch.cuda.synchronize()
+    agree = bool(torch.allclose(out, y_plan, rtol=1e-5, atol=1e-6))
+    cbm_mkl_cpp.check_device()
+    del out
+    return {"call": "cbm_mkl_cpp.s_spmm_fused_update_csr_int32 on CUDA tensors (the reference's operator "
+                    "signature, stateless GPU product)",
+            "ms": ms, "value": b_alg / (ms * 1e-3) / 1e9, "unit": "GB/s", "plan_ms": plan_ms,
+            "agrees_with_plan_rtol1e-5_atol1e-6": agree}
+
+
 def small_form(steps, warmup):
     """The 4,096-node community graph (64 communities of 64, 12 in-community
     and 4 uniform neighbours, seed 0, alpha 0): A.X with X FP32 U[-1, 1],
@@ -943,6 +976,10 @@ def main():
             line["gcn"] = gcn_timing(max(args.steps, 10), max(args.warmup, 3))
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(a, x.cpu().numpy(), b_alg)
+        if world == 1 and not args.no_forms:
+            # y holds the plan product of x (the last step of the e2e leg wrote
+            # y_host, not y)
+            line["direct"] = _form(lambda: direct_form(a, x, y, b_alg, kernel_ms, max(args.steps, 10), args.warmup))
         if world == 1 and not args.no_forms:
             del xh, yh, x, y, a
             torch.cuda.empty_cache()
