@@ -601,14 +601,17 @@ def run_precision(args):
     print(json.dumps(line), flush=True)
 
 
-def direct_form(a, x, y_plan, b_alg, plan_ms, steps, warmup):
+def direct_form(a, x, y_plan, b_alg, plan_ms, steps, warmup, ei, n):
     """The reference's CPU operator s_spmm_fused_update_csr_int32
     (cbm/cbm_extensions.cpp:593-698) through its own signature on CUDA tensors
     (csrc/direct.cu: no plan; the caller's CSR and tree arrays read as given),
     on the headline's structure, prepared values, multipliers and X: ms per
-    product at the headline's algorithmic bytes, beside the plan path, and its
-    agreement with the plan path's result (rtol 1e-5, atol 1e-6: its update
-    rounds as the CPU code does, fma(Y[u], m[v] / m[u], Y[v]))."""
+    product at the headline's algorithmic bytes, beside the plan path; its
+    error against FP64 on sampled rows, and its largest difference from the
+    plan path's result.  The two sum a row's entries in different orders
+    (one sequential chain here, chunk partials added in order for the plan's
+    long rows) and round the update differently (fma(Y[u], m[v] / m[u], Y[v])
+    here, as the CPU code does), so they agree to rounding, not bit for bit."""
     from cbm import cbm_mkl_cpp
 
     crow = a.deltas.crow_indices()
@@ -623,13 +626,15 @@ def direct_form(a, x, y_plan, b_alg, plan_ms, steps, warmup):
     ms = _time_events(run, steps, warmup)
     run()
     torch.cuda.synchronize()
-    agree = bool(torch.allclose(out, y_plan, rtol=1e-5, atol=1e-6))
     cbm_mkl_cpp.check_device()
+    max_diff = float((out - y_plan).abs().max())
+    dinv = dinv_f64(ei, n)
+    err = fp64_sample_error(ei, n, x, out, rs=dinv, cs=dinv)
     del out
     return {"call": "cbm_mkl_cpp.s_spmm_fused_update_csr_int32 on CUDA tensors (the reference's operator "
                     "signature, stateless GPU product)",
             "ms": ms, "value": b_alg / (ms * 1e-3) / 1e9, "unit": "GB/s", "plan_ms": plan_ms,
-            "agrees_with_plan_rtol1e-5_atol1e-6": agree}
+            "error_vs_fp64": err, "max_abs_diff_vs_plan": max_diff}
 
 
 def small_form(steps, warmup):
@@ -979,7 +984,8 @@ def main():
         if world == 1 and not args.no_forms:
             # y holds the plan product of x (the last step of the e2e leg wrote
             # y_host, not y)
-            line["direct"] = _form(lambda: direct_form(a, x, y, b_alg, kernel_ms, max(args.steps, 10), args.warmup))
+            line["direct"] = _form(lambda: direct_form(a, x, y, b_alg, kernel_ms, max(args.steps, 10), args.warmup,
+                                                       ei, n))
         if world == 1 and not args.no_forms:
             del xh, yh, x, y, a
             torch.cuda.empty_cache()
