@@ -95,7 +95,7 @@ __global__ void __launch_bounds__(kDirectThreads) direct_mark(const DirectArgs a
 // Team of TL lanes per row; lane owns VPL vectors of V floats per pass of
 // TL * VPL * V columns.
 template <int TL, int VPL, int V>
-__global__ void __launch_bounds__(kDirectThreads) direct_spmm(const DirectArgs a) {
+__global__ void __launch_bounds__(kDirectThreads, 4) direct_spmm(const DirectArgs a) {
   constexpr int kTeams = kDirectThreads / TL;
   constexpr int U = (VPL * V >= 8) ? 4 : 8;  // entries whose gathers are in flight together
   constexpr int64_t kPass = (int64_t)TL * VPL * V;
@@ -113,6 +113,22 @@ __global__ void __launch_bounds__(kDirectThreads) direct_spmm(const DirectArgs a
       for (int q = 0; q < VPL; ++q)
 #pragma unroll
         for (int j = 0; j < V; ++j) acc[q][j] = 0.f;
+      // wide rows (groups of 4): the next group's columns and values are
+      // loaded while the current group's X rows are gathered; narrow rows
+      // (groups of 8) load each group's own at its start, which keeps their
+      // registers within four blocks per SM
+      constexpr bool kPrefetch = U == 4;
+      int32_t pc[U];
+      float pw[U];
+      auto fetch = [&](int64_t k) {
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const bool in = k + u < e;
+          pc[u] = in ? __ldg(a.col + k + u) : 0;
+          pw[u] = (in && a.val) ? __ldg(a.val + k + u) : 1.f;
+        }
+      };
+      if (kPrefetch && b < e) fetch(b);
       for (int64_t k0 = b; k0 < e; k0 += U) {
         const int n = (int)((e - k0) < U ? (e - k0) : U);
         int64_t off[U];
@@ -122,15 +138,16 @@ __global__ void __launch_bounds__(kDirectThreads) direct_spmm(const DirectArgs a
           off[u] = -1;
           w[u] = 0.f;
           if (u < n) {
-            const int32_t cj = __ldg(a.col + k0 + u);
+            const int32_t cj = kPrefetch ? pc[u] : __ldg(a.col + k0 + u);
             if (cj < 0 || cj >= a.n_cols) {
               if (tl == 0) record(a.qs, CBM_ERR_INDEX, k0 + u);
             } else {
               off[u] = (int64_t)cj * a.c;
-              w[u] = a.val ? __ldg(a.val + k0 + u) : 1.f;
+              w[u] = kPrefetch ? pw[u] : (a.val ? __ldg(a.val + k0 + u) : 1.f);
             }
           }
         }
+        if (kPrefetch && k0 + U < e) fetch(k0 + U);
         float xv[U][VPL][V];
 #pragma unroll
         for (int u = 0; u < U; ++u)
