@@ -213,6 +213,10 @@ class Plan:
         key = (cols, x.dtype, y.dtype)
         bufs = getattr(self, "_host_bufs", {})
         if key not in bufs:
+            if bufs:
+                # copies of earlier calls may still use the old buffers
+                self.host_wait()
+                torch.cuda.current_stream(self.device).synchronize()
             bufs.clear()
             bufs[key] = (torch.empty(self.n_cols, cols, dtype=x.dtype, device=self.device),
                          torch.empty(self.n_rows, cols, dtype=y.dtype, device=self.device))

@@ -607,7 +607,10 @@ int cbm_matmul_host(cbm_plan* P, int32_t op, const void* x_host, int32_t xdt, in
   if (!(overlap && P->host_prev_valid)) {
     if (cudaStreamWaitEvent(P->h2d, ev[0], 0) != cudaSuccess) return CBM_ERR_CUDA;
   } else if (!same_layout) {
+    // other buffers or slabs: after the previous call's products and its
+    // pending copy-out (the new device buffers may reuse its memory)
     if (cudaStreamWaitEvent(P->h2d, P->host_prev_prod, 0) != cudaSuccess) return CBM_ERR_CUDA;
+    if (P->host_out_pending && cudaStreamWaitEvent(P->h2d, ev[1], 0) != cudaSuccess) return CBM_ERR_CUDA;
   }
   // a previous call's copy-out still pending: the products may not overwrite
   // the device copy of Y before it has left (slab by slab with the same layout)
